@@ -1,0 +1,1034 @@
+// engine.cu -- host side of the device PDLP engine: validation, layout,
+// device arena, setup kernels, the graph-captured iteration loop and result
+// extraction. Restates the control of PdlpSolver::solve
+// (pdlp_engine/src/pdlp_solver.cpp:116-548) for a batch of instances whose
+// per-iteration decisions all happen on the device.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <thread>
+
+namespace pdlpgpu {
+
+const char* message_text(int32_t id) {
+    switch (id) {
+        case kMsgInitialOptimal: return "Initial point satisfies the requested tolerances";
+        case kMsgNonFinite: return "PDHG generated a non-finite iterate";
+        case kMsgLinesearch: return "Adaptive linesearch failed to accept a step";
+        case kMsgInfeasible: return "Primal infeasible: Farkas ray found";
+        case kMsgUnbounded: return "Unbounded: improving ray found";
+        case kMsgOptimal: return "Primal, dual, and gap tolerances satisfied";
+        case kMsgPolishOptimal: return "Tolerances satisfied after refinement polishing";
+        case kMsgIterationLimit: return "Iteration limit reached";
+        case kMsgTimeLimit: return "Time limit reached";
+        default: return "";
+    }
+}
+
+namespace {
+
+struct ArenaPlan {
+    struct Req { void** ptr; size_t bytes; };
+    std::vector<Req> reqs;
+    template <class T>
+    void add(T*& p, int64_t count) {
+        reqs.push_back(Req{reinterpret_cast<void**>(&p), static_cast<size_t>(std::max<int64_t>(count, 1)) * sizeof(T)});
+    }
+    template <class T>
+    void add(const T*& p, int64_t count) {
+        reqs.push_back(Req{reinterpret_cast<void**>(const_cast<T**>(&p)), static_cast<size_t>(std::max<int64_t>(count, 1)) * sizeof(T)});
+    }
+    size_t total() const {
+        size_t t = 0;
+        for (const Req& r : reqs) t += (r.bytes + 255) & ~size_t(255);
+        return t;
+    }
+    void assign(char* base) const {
+        size_t off = 0;
+        for (const Req& r : reqs) {
+            *r.ptr = base + off;
+            off += (r.bytes + 255) & ~size_t(255);
+        }
+    }
+};
+
+double clampd(double v, double lo, double hi) { return v < lo ? lo : (hi < v ? hi : v); }
+
+// TerminationChecker's normalisers (termination.cpp:14-62), in the
+// reference's summation order.
+void normalisers(const pdlpgpu_lp& lp, double& pnorm, double& dnorm) {
+    double sum = 0.0;
+    for (int32_t i = 0; i < lp.num_rows; ++i) {
+        const double l = lp.row_lower[i], u = lp.row_upper[i];
+        if (std::isfinite(l)) sum += l * l;
+        if (std::isfinite(u) && u != l) sum += u * u;
+    }
+    pnorm = 1.0 + std::sqrt(sum);
+    double cs = 0.0;
+    for (int32_t j = 0; j < lp.num_cols; ++j) cs += lp.objective[j] * lp.objective[j];
+    dnorm = 1.0 + std::sqrt(cs);
+}
+
+template <class T>
+void fill_value(std::vector<T>& v, size_t n, T x) { v.assign(n, x); }
+
+}  // namespace
+
+Engine::Engine(int device) : device_(device) {}
+
+Engine::~Engine() {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    if (arena_) cudaFree(arena_);
+    if (h_active_) cudaFreeHost(h_active_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+bool Engine::check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    if (error_.empty()) error_ = std::string(what) + ": " + cudaGetErrorString(e);
+    return false;
+}
+
+template <class V>
+void Engine::to_internal_cols(const V* src, std::vector<V>& dst, int b) const {
+    const MatrixLayout& L = layouts_[spec_.shared_matrix ? 0 : b];
+    dst.resize(L.col_perm.size());
+    for (size_t c = 0; c < L.col_perm.size(); ++c) dst[c] = src[L.col_perm[c]];
+}
+
+template <class V>
+void Engine::to_internal_rows(const V* src, std::vector<V>& dst, int b) const {
+    const MatrixLayout& L = layouts_[spec_.shared_matrix ? 0 : b];
+    dst.resize(L.row_perm.size());
+    for (size_t r = 0; r < L.row_perm.size(); ++r) dst[r] = src[L.row_perm[r]];
+}
+
+bool Engine::prepare(const SolveSpec& spec) {
+    t0_ = std::chrono::steady_clock::now();
+    spec_ = spec;
+    const int nspec = static_cast<int>(spec.lps.size());
+    invalid_.assign(static_cast<size_t>(nspec), std::string());
+    device_of_.assign(static_cast<size_t>(nspec), -1);
+    const pdlpgpu_options& o = spec.opt;
+    mixed_ = spec.ext.precision == PDLPGPU_PRECISION_MIXED;
+
+    // --- host validation (pdlp_solver.cpp:121-134) -----------------------
+    std::vector<HostCsr> csr(static_cast<size_t>(spec.shared_matrix ? 1 : nspec));
+    std::string shared_error;
+    if (spec.shared_matrix && nspec > 0) shared_error = canonicalize(*spec.lps[0], csr[0]);
+    for (int i = 0; i < nspec; ++i) {
+        const pdlpgpu_lp& lp = *spec.lps[i];
+        std::string err;
+        if (spec.shared_matrix) {
+            err = shared_error;
+            if (err.empty() && (lp.num_rows != spec.lps[0]->num_rows || lp.num_cols != spec.lps[0]->num_cols))
+                err = "CompiledLp row vector dimensions do not match A";
+        } else {
+            err = canonicalize(lp, csr[i]);
+        }
+        if (err.empty()) err = validate_vectors(lp);
+        invalid_[i] = err;
+    }
+    const bool bad_options = o.iteration_limit < 0 || o.termination_check_frequency <= 0 ||
+                             o.primal_tolerance < 0.0 || o.dual_tolerance < 0.0 ||
+                             o.gap_tolerance < 0.0 || o.initial_step_safety <= 0.0 ||
+                             o.minimum_primal_weight <= 0.0 ||
+                             o.maximum_primal_weight < o.minimum_primal_weight;
+    for (int i = 0; i < nspec; ++i) {
+        if (invalid_[i].empty() && bad_options) invalid_[i] = "Invalid PDLP options";
+        if (invalid_[i].empty()) device_of_[i] = count_++;
+    }
+    if (count_ == 0) {
+        setup_ok_ = true;
+        return true;
+    }
+
+    // --- device and tuning ------------------------------------------------
+    if (!check(cudaSetDevice(device_), "cudaSetDevice")) return false;
+    cudaDeviceProp prop;
+    if (!check(cudaGetDeviceProperties(&prop, device_), "cudaGetDeviceProperties")) return false;
+    sms_ = prop.multiProcessorCount;
+    if (!check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
+
+    // Layouts: one per device instance, or one shared.
+    std::vector<HostCsr> csrT;
+    std::vector<int> spec_of(static_cast<size_t>(count_));
+    for (int i = 0; i < nspec; ++i) if (device_of_[i] >= 0) spec_of[device_of_[i]] = i;
+    const int nlayouts = spec.shared_matrix ? 1 : count_;
+    {
+        int64_t nnz = 0, lines = 0, clines = 0;
+        for (int k = 0; k < nlayouts; ++k) {
+            const HostCsr& a = csr[spec.shared_matrix ? 0 : spec_of[k]];
+            nnz += a.nnz();
+            lines += a.rows;
+            clines += a.cols;
+        }
+        HostCsr agg_a, agg_at;   // only the counts matter for the heuristic
+        agg_a.rows = static_cast<int32_t>(std::min<int64_t>(lines, INT32_MAX));
+        agg_at.rows = static_cast<int32_t>(std::min<int64_t>(clines, INT32_MAX));
+        agg_a.value.resize(0);
+        tuning_ = Tuning();
+        const double mean_a = lines ? static_cast<double>(nnz) / lines : 0.0;
+        const double mean_at = clines ? static_cast<double>(nnz) / clines : 0.0;
+        const double mean = std::min(mean_a, mean_at);
+        // Wider lane loads pay only when lines are long enough that rounding
+        // each slice's steps up to the width adds little padding.
+        if (mixed_) tuning_.vector_width = mean >= 24.0 ? 4 : (mean >= 12.0 ? 2 : 1);
+        else tuning_.vector_width = mean >= 16.0 ? 2 : 1;
+        if (spec.ext.lane_elements > 0) tuning_.lane_elements = spec.ext.lane_elements;
+        if (spec.ext.vector_width == 1 || spec.ext.vector_width == 2 || spec.ext.vector_width == 4)
+            tuning_.vector_width = spec.ext.vector_width;
+    }
+    layouts_.resize(static_cast<size_t>(nlayouts));
+    {
+        auto build = [&](int k) {
+            const HostCsr& a = csr[spec.shared_matrix ? 0 : spec_of[k]];
+            const HostCsr at = transpose(a);
+            layouts_[k] = build_layout(a, at, tuning_);
+        };
+        const int threads = std::min<int>(nlayouts, std::max(1u, std::thread::hardware_concurrency()));
+        if (threads <= 1) {
+            for (int k = 0; k < nlayouts; ++k) build(k);
+        } else {
+            std::vector<std::thread> pool;
+            for (int t = 0; t < threads; ++t)
+                pool.emplace_back([&, t] { for (int k = t; k < nlayouts; k += threads) build(k); });
+            for (auto& th : pool) th.join();
+        }
+    }
+    if (!csr.empty()) csr0_ = std::move(csr[spec.shared_matrix ? 0 : spec_of[0]]);
+    csr.clear();
+
+    // --- spaces, slices and CTA maps --------------------------------------
+    info_.resize(static_cast<size_t>(count_));
+    rows_total_ = cols_total_ = 0;
+    a_slots_ = at_slots_ = 0;
+    a_slices_ = at_slices_ = 0;
+    for (int k = 0; k < nlayouts; ++k) {
+        a_slots_ += layouts_[k].a.slots();
+        at_slots_ += layouts_[k].at.slots();
+        a_slices_ += static_cast<int32_t>(layouts_[k].a.slices.size());
+        at_slices_ += static_cast<int32_t>(layouts_[k].at.slices.size());
+    }
+    const int64_t target_a = cta_target_slots(spec.shared_matrix ? a_slots_ * count_ : a_slots_, sms_);
+    const int64_t target_at = cta_target_slots(spec.shared_matrix ? at_slots_ * count_ : at_slots_, sms_);
+    a_ctas_.clear();
+    at_ctas_.clear();
+    vec_.clear();
+    int64_t a_data = 0, at_data = 0;
+    int32_t a_sl = 0, at_sl = 0;
+    for (int b = 0; b < count_; ++b) {
+        const MatrixLayout& L = layouts_[spec.shared_matrix ? 0 : b];
+        InstanceInfo& inf = info_[b];
+        inf.m = L.m;
+        inf.n = L.n;
+        inf.row_off = rows_total_;
+        inf.col_off = cols_total_;
+        rows_total_ += L.m;
+        cols_total_ += L.n;
+        const bool own = !spec.shared_matrix || b == 0;
+        inf.a_data_base = spec.shared_matrix ? 0 : a_data;
+        inf.at_data_base = spec.shared_matrix ? 0 : at_data;
+        inf.a_slice_base = spec.shared_matrix ? 0 : a_sl;
+        inf.at_slice_base = spec.shared_matrix ? 0 : at_sl;
+        inf.a_len_base = spec.shared_matrix ? 0 : inf.row_off;
+        inf.at_len_base = spec.shared_matrix ? 0 : inf.col_off;
+        if (own && !spec.shared_matrix) {
+            a_data += L.a.slots();
+            at_data += L.at.slots();
+            a_sl += static_cast<int32_t>(L.a.slices.size());
+            at_sl += static_cast<int32_t>(L.at.slices.size());
+        }
+        inf.a_cta_begin = static_cast<int32_t>(a_ctas_.size());
+        append_cta_map(L.a, b, inf.a_slice_base, target_a, a_ctas_);
+        inf.a_cta_end = static_cast<int32_t>(a_ctas_.size());
+        inf.at_cta_begin = static_cast<int32_t>(at_ctas_.size());
+        append_cta_map(L.at, b, inf.at_slice_base, target_at, at_ctas_);
+        inf.at_cta_end = static_cast<int32_t>(at_ctas_.size());
+        inf.vec_cta_begin = static_cast<int32_t>(vec_.size());
+        append_vec_map(b, L.m, L.n, vec_);
+        inf.vec_cta_end = static_cast<int32_t>(vec_.size());
+    }
+    first_a_ctas_ = info_[0].a_cta_end - info_[0].a_cta_begin;
+    first_at_ctas_ = info_[0].at_cta_end - info_[0].at_cta_begin;
+    first_vec_ = info_[0].vec_cta_end - info_[0].vec_cta_begin;
+
+    // --- device arena ------------------------------------------------------
+    const int64_t R = rows_total_, N = cols_total_;
+    const int64_t slots = a_slots_ + at_slots_;
+    const int64_t lens = spec.shared_matrix ? (layouts_[0].m + layouts_[0].n) : (R + N);
+    bool any_warm = false;
+    for (const auto* w : spec.warm) any_warm |= (w != nullptr && (w->primal || w->row_dual));
+    ArenaPlan plan;
+    SliceDesc* d_slices = nullptr;
+    int32_t* d_idx = nullptr;
+    double* d_val = nullptr;
+    int32_t* d_len = nullptr;
+    CtaWork* d_ctas = nullptr;
+    VecWork* d_vec = nullptr;
+    InstanceInfo* d_info = nullptr;
+    double* warm_x = nullptr;
+    double* warm_y = nullptr;
+    plan.add(d_slices, a_slices_ + at_slices_);
+    plan.add(d_idx, slots);
+    plan.add(d_val, slots);
+    plan.add(a_s64_, a_slots_);
+    plan.add(at_s64_, at_slots_);
+    if (mixed_) {
+        plan.add(a_s32_, a_slots_);
+        plan.add(at_s32_, at_slots_);
+    }
+    plan.add(d_len, lens);
+    plan.add(d_ctas, static_cast<int64_t>(a_ctas_.size() + at_ctas_.size()));
+    plan.add(d_vec, static_cast<int64_t>(vec_.size()));
+    plan.add(d_info, count_);
+    plan.add(g_.ctl, count_);
+    for (double** p : {&g_.rs, &g_.row_tmp, &g_.y_o, &g_.ya_o, &g_.dy_o, &g_.best_y, &g_.dray}) plan.add(*p, R);
+    for (double** p : {&g_.cs, &g_.col_tmp, &g_.x_o, &g_.xa_o, &g_.p_proj, &g_.best_x, &g_.pray}) plan.add(*p, N);
+    plan.add(g_.c_orig, N);
+    plan.add(g_.xl_orig, N);
+    plan.add(g_.xu_orig, N);
+    plan.add(g_.rl_orig, R);
+    plan.add(g_.ru_orig, R);
+    if (any_warm) {
+        plan.add(warm_x, N);
+        plan.add(warm_y, R);
+    }
+    plan.add(g_.part_primal, static_cast<int64_t>(at_ctas_.size()));
+    plan.add(g_.part_dual, 2 * static_cast<int64_t>(a_ctas_.size()));
+    plan.add(g_.part_prep, kPrepSlots * static_cast<int64_t>(vec_.size()));
+    plan.add(g_.part_check, kCheckSlots * static_cast<int64_t>(a_ctas_.size() + at_ctas_.size()));
+    plan.add(g_.count_dual, count_);
+    plan.add(g_.count_check, count_);
+    plan.add(d_active_, 1);
+    auto plan_work = [&](auto& w, int64_t Rn, int64_t Nn) {
+        for (int k = 0; k < 2; ++k) {
+            plan.add(w.X[k], Nn);
+            plan.add(w.Y[k], Rn);
+            plan.add(w.AX[k], Rn);
+        }
+        for (auto** p : {&w.avg_x, &w.rx, &w.c, &w.xl, &w.xu, &w.tau, &w.itau}) plan.add(*p, Nn);
+        for (auto** p : {&w.avg_y, &w.ry, &w.rl, &w.ru, &w.sigma, &w.isigma}) plan.add(*p, Rn);
+    };
+    plan_work(w64_, R, N);
+    if (mixed_) plan_work(w32_, R, N);
+    arena_bytes_ = plan.total();
+    if (!check(cudaMalloc(&arena_, arena_bytes_), "cudaMalloc")) return false;
+    plan.assign(arena_);
+    if (!check(cudaMallocHost(&h_active_, sizeof(int32_t)), "cudaMallocHost")) return false;
+    if (!check(cudaMemsetAsync(arena_, 0, arena_bytes_, stream_), "cudaMemset")) return false;
+
+    // --- host staging and upload ------------------------------------------
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes == 0) return true;
+        return check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_), "upload");
+    };
+    {
+        std::vector<SliceDesc> slices;
+        slices.reserve(static_cast<size_t>(a_slices_ + at_slices_));
+        std::vector<int32_t> idx;
+        std::vector<double> val;
+        idx.reserve(static_cast<size_t>(slots));
+        val.reserve(static_cast<size_t>(slots));
+        for (int k = 0; k < nlayouts; ++k) {
+            slices.insert(slices.end(), layouts_[k].a.slices.begin(), layouts_[k].a.slices.end());
+            idx.insert(idx.end(), layouts_[k].a.idx.begin(), layouts_[k].a.idx.end());
+            val.insert(val.end(), layouts_[k].a.val.begin(), layouts_[k].a.val.end());
+        }
+        for (int k = 0; k < nlayouts; ++k) {
+            slices.insert(slices.end(), layouts_[k].at.slices.begin(), layouts_[k].at.slices.end());
+            idx.insert(idx.end(), layouts_[k].at.idx.begin(), layouts_[k].at.idx.end());
+            val.insert(val.end(), layouts_[k].at.val.begin(), layouts_[k].at.val.end());
+        }
+        if (!up(d_slices, slices.data(), slices.size() * sizeof(SliceDesc))) return false;
+        if (!up(d_idx, idx.data(), idx.size() * sizeof(int32_t))) return false;
+        if (!up(d_val, val.data(), val.size() * sizeof(double))) return false;
+        std::vector<int32_t> len;
+        len.reserve(static_cast<size_t>(lens));
+        for (int k = 0; k < nlayouts; ++k) len.insert(len.end(), layouts_[k].a.line_len.begin(), layouts_[k].a.line_len.end());
+        const size_t a_len_total = len.size();
+        for (int k = 0; k < nlayouts; ++k) len.insert(len.end(), layouts_[k].at.line_len.begin(), layouts_[k].at.line_len.end());
+        if (!up(d_len, len.data(), len.size() * sizeof(int32_t))) return false;
+        std::vector<CtaWork> ctas(a_ctas_);
+        ctas.insert(ctas.end(), at_ctas_.begin(), at_ctas_.end());
+        if (!up(d_ctas, ctas.data(), ctas.size() * sizeof(CtaWork))) return false;
+        if (!up(d_vec, vec_.data(), vec_.size() * sizeof(VecWork))) return false;
+        if (!up(d_info, info_.data(), info_.size() * sizeof(InstanceInfo))) return false;
+        // Wire the sides: A-side data first, then A^T-side data.
+        g_.a.slices = d_slices;
+        g_.at.slices = d_slices + a_slices_;
+        g_.a.idx = d_idx;
+        g_.at.idx = d_idx + a_slots_;
+        g_.a.val_orig = d_val;
+        g_.at.val_orig = d_val + a_slots_;
+        g_.a.val_s64 = a_s64_;
+        g_.at.val_s64 = at_s64_;
+        g_.a.val_s32 = a_s32_;
+        g_.at.val_s32 = at_s32_;
+        g_.a.line_len = d_len;
+        g_.at.line_len = d_len + a_len_total;
+        g_.a.ctas = d_ctas;
+        g_.at.ctas = d_ctas + a_ctas_.size();
+        g_.a.num_ctas = static_cast<int32_t>(a_ctas_.size());
+        g_.at.num_ctas = static_cast<int32_t>(at_ctas_.size());
+        g_.vec = d_vec;
+        g_.num_vec = static_cast<int32_t>(vec_.size());
+        g_.info = d_info;
+        g_.shared_matrix = spec.shared_matrix ? 1 : 0;
+        g_.warm_x = nullptr;
+        g_.warm_y = nullptr;
+        // A^T-side data bases, slice indices and line bases in info_ and in the
+        // CTA map are relative to the g_.at pointers.
+    }
+    {
+        // Original-problem vectors in internal order.
+        std::vector<double> cvec(static_cast<size_t>(N)), xl(static_cast<size_t>(N)), xu(static_cast<size_t>(N));
+        std::vector<double> rl(static_cast<size_t>(R)), ru(static_cast<size_t>(R));
+        std::vector<double> wx, wy;
+        if (any_warm) {
+            wx.assign(static_cast<size_t>(N), std::nan(""));
+            wy.assign(static_cast<size_t>(R), std::nan(""));
+        }
+        std::vector<double> tmp;
+        for (int i = 0; i < nspec; ++i) {
+            const int b = device_of_[i];
+            if (b < 0) continue;
+            const pdlpgpu_lp& lp = *spec.lps[i];
+            const InstanceInfo& inf = info_[b];
+            to_internal_cols(lp.objective, tmp, b);
+            std::copy(tmp.begin(), tmp.end(), cvec.begin() + inf.col_off);
+            to_internal_cols(lp.var_lower, tmp, b);
+            std::copy(tmp.begin(), tmp.end(), xl.begin() + inf.col_off);
+            to_internal_cols(lp.var_upper, tmp, b);
+            std::copy(tmp.begin(), tmp.end(), xu.begin() + inf.col_off);
+            to_internal_rows(lp.row_lower, tmp, b);
+            std::copy(tmp.begin(), tmp.end(), rl.begin() + inf.row_off);
+            to_internal_rows(lp.row_upper, tmp, b);
+            std::copy(tmp.begin(), tmp.end(), ru.begin() + inf.row_off);
+            const pdlpgpu_warmstart* w = (i < static_cast<int>(spec.warm.size())) ? spec.warm[i] : nullptr;
+            if (w && w->primal) {
+                to_internal_cols(w->primal, tmp, b);
+                std::copy(tmp.begin(), tmp.end(), wx.begin() + inf.col_off);
+            }
+            if (w && w->row_dual) {
+                to_internal_rows(w->row_dual, tmp, b);
+                std::copy(tmp.begin(), tmp.end(), wy.begin() + inf.row_off);
+            }
+        }
+        if (!up(const_cast<double*>(g_.c_orig), cvec.data(), cvec.size() * 8)) return false;
+        if (!up(const_cast<double*>(g_.xl_orig), xl.data(), xl.size() * 8)) return false;
+        if (!up(const_cast<double*>(g_.xu_orig), xu.data(), xu.size() * 8)) return false;
+        if (!up(const_cast<double*>(g_.rl_orig), rl.data(), rl.size() * 8)) return false;
+        if (!up(const_cast<double*>(g_.ru_orig), ru.data(), ru.size() * 8)) return false;
+        if (any_warm) {
+            // NaN marks "no warm value": k_setup_vectors falls back to the cold point.
+            if (!up(warm_x, wx.data(), wx.size() * 8)) return false;
+            if (!up(warm_y, wy.data(), wy.size() * 8)) return false;
+            g_.warm_x = warm_x;
+            g_.warm_y = warm_y;
+        }
+        std::vector<double> ones(static_cast<size_t>(std::max(R, N)), 1.0);
+        if (!up(g_.rs, ones.data(), static_cast<size_t>(R) * 8)) return false;
+        if (!up(g_.cs, ones.data(), static_cast<size_t>(N) * 8)) return false;
+        // Preconditioner defaults (disabled preconditioning keeps these).
+        if (!up(w64_.tau, ones.data(), static_cast<size_t>(N) * 8)) return false;
+        if (!up(w64_.itau, ones.data(), static_cast<size_t>(N) * 8)) return false;
+        if (!up(w64_.sigma, ones.data(), static_cast<size_t>(R) * 8)) return false;
+        if (!up(w64_.isigma, ones.data(), static_cast<size_t>(R) * 8)) return false;
+        if (mixed_) {
+            std::vector<float> f1(static_cast<size_t>(std::max(R, N)), 1.0f);
+            if (!up(w32_.tau, f1.data(), static_cast<size_t>(N) * 4)) return false;
+            if (!up(w32_.itau, f1.data(), static_cast<size_t>(N) * 4)) return false;
+            if (!up(w32_.sigma, f1.data(), static_cast<size_t>(R) * 4)) return false;
+            if (!up(w32_.isigma, f1.data(), static_cast<size_t>(R) * 4)) return false;
+        }
+    }
+
+    // --- options and per-instance control ---------------------------------
+    dopt_.iteration_limit = o.iteration_limit;
+    dopt_.check_frequency = o.termination_check_frequency;
+    dopt_.max_trials = std::max(o.maximum_step_trials, 1);
+    dopt_.adaptive = o.use_adaptive_linesearch != 0;
+    dopt_.averaging = o.use_averaging != 0;
+    dopt_.restarts = o.use_restarts != 0;
+    dopt_.detect_infeasibility = o.detect_infeasibility != 0;
+    dopt_.polishing = o.use_feasibility_polishing != 0;
+    dopt_.polishing_iterations = o.polishing_iterations;
+    dopt_.min_restart = o.minimum_restart_iterations;
+    dopt_.max_restart = o.maximum_restart_iterations;
+    dopt_.mixed = mixed_ ? 1 : 0;
+    dopt_.fp32_stall_checks = spec.ext.fp32_stall_checks > 0 ? spec.ext.fp32_stall_checks : 8;
+    dopt_.primal_tol = o.primal_tolerance;
+    dopt_.dual_tol = o.dual_tolerance;
+    dopt_.gap_tol = o.gap_tolerance;
+    dopt_.min_step_scale = o.minimum_step_scale;
+    dopt_.w_min = o.minimum_primal_weight;
+    dopt_.w_max = o.maximum_primal_weight;
+    dopt_.smoothing = o.primal_weight_smoothing;
+    dopt_.initial_step_safety = o.initial_step_safety;
+    dopt_.sufficient = o.restart_sufficient_decay;
+    dopt_.necessary = o.restart_necessary_decay;
+    dopt_.artificial = o.restart_artificial_fraction;
+    dopt_.infeasibility_tol = o.infeasibility_tolerance;
+    dopt_.time_limit = o.time_limit_seconds;
+    setup_ok_ = true;
+    return true;
+}
+
+
+// ---------------------------------------------------------------------------
+// Control state, setup kernels, initial check
+// ---------------------------------------------------------------------------
+bool Engine::init_control() {
+    const pdlpgpu_options& o = spec_.opt;
+    std::vector<InstanceCtl> ctl(static_cast<size_t>(count_));
+    for (size_t i = 0; i < spec_.lps.size(); ++i) {
+        const int b = device_of_[i];
+        if (b < 0) continue;
+        const pdlpgpu_lp& lp = *spec_.lps[i];
+        InstanceCtl c;
+        std::memset(&c, 0, sizeof(c));
+        c.phase = kPhaseMain;
+        c.stage = kStageCheck;
+        c.check_kind = kCheckInitial;
+        c.need_refresh = 1;
+        c.fp64_stage = mixed_ ? 0 : 1;
+        c.status = -1;
+        c.limit_status = 3;
+        const pdlpgpu_warmstart* w = i < spec_.warm.size() ? spec_.warm[i] : nullptr;
+        const bool warm = w != nullptr && (w->primal != nullptr || w->row_dual != nullptr);
+        c.have_avg_at_check = warm ? 1 : 0;
+        // StepController (step_controller.cpp:17-28) with the preconditioned
+        // static bound 0.99 (pdlp_solver.cpp:188); the power iteration
+        // replaces it when preconditioning is off.
+        c.eta_max = 0.99;
+        c.eta = clampd(o.initial_step_safety * c.eta_max, o.minimum_step_scale * c.eta_max, c.eta_max);
+        c.omega = 1.0;
+        auto set_w = [&](double v) {
+            if (v > 0.0 && std::isfinite(v)) c.omega = clampd(v, o.minimum_primal_weight, o.maximum_primal_weight);
+        };
+        set_w(o.initial_primal_weight);
+        if (w != nullptr && w->primal_weight > 0.0) set_w(w->primal_weight);
+        c.trial_eta = c.eta;
+        c.trial_omega = c.omega;
+        c.ctl_eta = c.eta;
+        c.ctl_omega = c.omega;
+        c.best_pobj = std::nan("");
+        c.best_dobj = -INFINITY;
+        c.best_pres = c.best_dres = c.best_gap = c.best_kkt = INFINITY;
+        c.restart_baseline = INFINITY;
+        c.prev_candidate = INFINITY;
+        normalisers(lp, c.pnorm, c.dnorm);
+        c.objective_offset = lp.objective_offset;
+        ctl[static_cast<size_t>(b)] = c;
+    }
+    return check(cudaMemcpyAsync(g_.ctl, ctl.data(), ctl.size() * sizeof(InstanceCtl),
+                                 cudaMemcpyHostToDevice, stream_), "upload control");
+}
+
+bool Engine::setup_kernels() {
+    const pdlpgpu_options& o = spec_.opt;
+    const int a_n = spec_.shared_matrix ? first_a_ctas_ : g_.a.num_ctas;
+    const int at_n = spec_.shared_matrix ? first_at_ctas_ : g_.at.num_ctas;
+    const int vec_n = spec_.shared_matrix ? first_vec_ : g_.num_vec;
+    const int V = tuning_.vector_width;
+    if (!spec_.working_given && o.use_ruiz_scaling && o.ruiz_iterations > 0) {
+        for (int pass = 0; pass < o.ruiz_iterations; ++pass) {
+            launch_ruiz_max(g_, V, a_n, at_n, stream_);
+            launch_ruiz_update(g_, vec_n, stream_);
+        }
+    }
+    launch_scale_values(g_, a_s64_, at_s64_, a_s32_, at_s32_, V, a_n, at_n, stream_);
+    if (spec_.shared_matrix) launch_broadcast_scales(g_, info_[0], count_, info_[0].m, info_[0].n, stream_);
+    if (o.use_diagonal_preconditioning) {
+        launch_precondition<double>(g_, w64_, 1, V, a_n, at_n, stream_);
+        if (mixed_) launch_precondition<float>(g_, w32_, 1, V, a_n, at_n, stream_);
+        if (spec_.shared_matrix) {
+            launch_broadcast_precond<double>(w64_, info_[0], count_, info_[0].m, info_[0].n, stream_);
+            if (mixed_) launch_broadcast_precond<float>(w32_, info_[0], count_, info_[0].m, info_[0].n, stream_);
+        }
+    }
+    launch_setup_vectors<double>(g_, w64_, stream_);
+    if (mixed_) launch_setup_vectors<float>(g_, w32_, stream_);
+    return check(cudaGetLastError(), "setup kernels");
+}
+
+// Power iteration on the scaled FP64 matrix (preconditioner.cpp:82-140). The
+// starting vector is the reference's: mt19937 seeded with 1, uniform on [-1, 1),
+// drawn in original column order.
+bool Engine::power_iteration() {
+    const pdlpgpu_options& o = spec_.opt;
+    std::vector<double> z(static_cast<size_t>(cols_total_));
+    std::vector<double> draw;
+    for (size_t i = 0; i < spec_.lps.size(); ++i) {
+        const int b = device_of_[i];
+        if (b < 0) continue;
+        const int32_t n = info_[b].n;
+        // MT19937 (Matsumoto and Nishimura, 1998); libstdc++ maps two draws
+        // to a double in [0, 1) before the affine map to [a, b).
+        uint32_t st[624];
+        st[0] = 1u;
+        for (int k = 1; k < 624; ++k) st[k] = 1812433253u * (st[k - 1] ^ (st[k - 1] >> 30)) + static_cast<uint32_t>(k);
+        int pos = 624;
+        auto next = [&]() {
+            if (pos >= 624) {
+                for (int k = 0; k < 624; ++k) {
+                    const uint32_t y = (st[k] & 0x80000000u) | (st[(k + 1) % 624] & 0x7fffffffu);
+                    st[k] = st[(k + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+                }
+                pos = 0;
+            }
+            uint32_t y = st[pos++];
+            y ^= y >> 11;
+            y ^= (y << 7) & 0x9d2c5680u;
+            y ^= (y << 15) & 0xefc60000u;
+            y ^= y >> 18;
+            return y;
+        };
+        draw.resize(static_cast<size_t>(n));
+        for (int32_t j = 0; j < n; ++j) {
+            double sum = 0.0, sc = 1.0;
+            for (int k = 0; k < 2; ++k) {
+                sum += static_cast<double>(next()) * sc;
+                sc *= 4294967296.0;
+            }
+            double r = sum / sc;
+            if (r >= 1.0) r = std::nextafter(1.0, 0.0);
+            draw[j] = r * 2.0 - 1.0;
+        }
+        std::vector<double> internal;
+        to_internal_cols(draw.data(), internal, b);
+        std::copy(internal.begin(), internal.end(), z.begin() + info_[b].col_off);
+    }
+    double* x = g_.x_o;
+    double* y = g_.y_o;
+    double* zd = g_.xa_o;
+    if (!check(cudaMemcpyAsync(zd, z.data(), z.size() * 8, cudaMemcpyHostToDevice, stream_), "upload power start"))
+        return false;
+    const int V = tuning_.vector_width;
+    launch_power_dot(g_, zd, zd, stream_);
+    launch_power_step(g_, count_, 1, 0, 1, stream_);
+    launch_power_scale(g_, x, zd, stream_);
+    const int budget = std::max(o.power_iteration_count, 1);
+    for (int it = 0; it < budget; ++it) {
+        launch_spmv<double>(g_, 0, 1, x, y, V, stream_);
+        launch_spmv<double>(g_, 1, 1, y, zd, V, stream_);
+        launch_power_dot(g_, x, zd, stream_);
+        launch_power_step(g_, count_, 0, it, budget, stream_);
+        launch_power_scale(g_, x, zd, stream_);
+    }
+    launch_power_finish(g_, count_, o.initial_step_safety, o.minimum_step_scale, stream_);
+    return check(cudaGetLastError(), "power iteration");
+}
+
+bool Engine::start() {
+    if (!setup_ok_) return false;
+    if (count_ == 0) return true;
+    if (!init_control()) return false;
+    if (!setup_kernels()) return false;
+    if (!spec_.opt.use_diagonal_preconditioning && !power_iteration()) return false;
+    const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
+    const double limit = spec_.opt.time_limit_seconds;
+    launch_stamp_clock(g_, count_, static_cast<int64_t>(elapsed * 1e9),
+                       limit > 0.0 ? static_cast<int64_t>(limit * 1e9) : 0, stream_);
+    // Initial A x (refresh is gated on need_refresh, set by init_control),
+    // then the initial score (pdlp_solver.cpp:239-264).
+    if (mixed_) launch_refresh<float>(g_, w32_, dopt_, tuning_.vector_width, stream_);
+    launch_refresh<double>(g_, w64_, dopt_, tuning_.vector_width, stream_);
+    enqueue_check_stage();
+    return check(cudaGetLastError(), "initial check");
+}
+
+// ---------------------------------------------------------------------------
+// The iteration loop
+// ---------------------------------------------------------------------------
+template <class T>
+void Engine::enqueue_trial(const Work<T>& w) {
+    launch_primal<T>(g_, w, dopt_, tuning_.vector_width, stream_);
+    launch_dual<T>(g_, w, dopt_, tuning_.vector_width, stream_);
+    launches_ += 2;
+}
+
+void Engine::enqueue_check_stage() {
+    const int V = tuning_.vector_width;
+    if (mixed_) launch_check_prep<float>(g_, w32_, dopt_, stream_);
+    launch_check_prep<double>(g_, w64_, dopt_, stream_);
+    launch_check_spmv(g_, dopt_, V, stream_);
+    if (mixed_) launch_check_apply<float>(g_, w32_, dopt_, stream_);
+    launch_check_apply<double>(g_, w64_, dopt_, stream_);
+    if (mixed_) launch_refresh<float>(g_, w32_, dopt_, V, stream_);
+    launch_refresh<double>(g_, w64_, dopt_, V, stream_);
+    cudaMemsetAsync(d_active_, 0, sizeof(int32_t), stream_);
+    launch_finalize(g_, count_, d_active_, stream_);
+    launches_ += mixed_ ? 8 : 5;
+}
+
+void Engine::enqueue_chunk(int slots) {
+    for (int k = 0; k < slots; ++k) {
+        if (mixed_) enqueue_trial<float>(w32_);
+        enqueue_trial<double>(w64_);
+    }
+    enqueue_check_stage();
+}
+
+bool Engine::build_graph(int slots) {
+    cudaGraph_t graph = nullptr;
+    if (!check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture"))
+        return false;
+    const int64_t before = launches_;
+    enqueue_chunk(slots);
+    launches_ = before;
+    if (!check(cudaStreamEndCapture(stream_, &graph), "end capture")) return false;
+    const bool ok = check(cudaGraphInstantiate(&graph_, graph, 0), "graph instantiate");
+    cudaGraphDestroy(graph);
+    graph_slots_ = slots;
+    return ok;
+}
+
+bool Engine::run() {
+    if (!setup_ok_ || count_ == 0) return setup_ok_;
+    const pdlpgpu_options& o = spec_.opt;
+    if (!check(cudaMemcpyAsync(h_active_, d_active_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "poll"))
+        return false;
+    if (!check(cudaStreamSynchronize(stream_), "setup")) return false;
+    const int slack = spec_.ext.chunk_slack > 0 ? spec_.ext.chunk_slack : 4;
+    const int slots = std::max(1, std::min(o.termination_check_frequency + slack, 1024));
+    const bool graphs = spec_.ext.disable_graphs == 0;
+    if (*h_active_ != 0 && graphs && !build_graph(slots)) return false;
+    const int per_chunk = (mixed_ ? 4 : 2) * slots + (mixed_ ? 8 : 5);
+    const int64_t trials_bound =
+        (std::max<int64_t>(o.iteration_limit, 0) + std::max(o.polishing_iterations, 0) + 2) *
+        std::max(o.maximum_step_trials, 1);
+    const int64_t max_chunks = trials_bound / std::max(1, slots - slack) + 64;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, stream_);
+    int64_t chunks = 0;
+    while (*h_active_ != 0) {
+        if (chunks >= max_chunks) {
+            error_ = "device loop exceeded its chunk bound";
+            break;
+        }
+        if (graphs) {
+            if (!check(cudaGraphLaunch(graph_, stream_), "graph launch")) break;
+            launches_ += per_chunk;
+        } else {
+            enqueue_chunk(slots);
+        }
+        ++chunks;
+        cudaMemcpyAsync(h_active_, d_active_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
+        if (!check(cudaStreamSynchronize(stream_), "iteration loop")) break;
+    }
+    cudaEventRecord(e1, stream_);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    device_seconds_ = 1e-3 * ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ran_ = true;
+    return error_.empty();
+}
+
+void Engine::results(std::vector<pdlpgpu_result*>& out) {
+    const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
+    std::vector<InstanceCtl> ctl(static_cast<size_t>(count_));
+    std::vector<double> bx, by, dr, pr;
+    bool have = false;
+    if (count_ > 0 && stream_ != nullptr && arena_ != nullptr) {
+        bx.resize(static_cast<size_t>(cols_total_));
+        by.resize(static_cast<size_t>(rows_total_));
+        dr.resize(static_cast<size_t>(rows_total_));
+        pr.resize(static_cast<size_t>(cols_total_));
+        have = check(cudaMemcpyAsync(ctl.data(), g_.ctl, ctl.size() * sizeof(InstanceCtl), cudaMemcpyDeviceToHost, stream_), "download") &&
+               check(cudaMemcpyAsync(bx.data(), g_.best_x, bx.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") &&
+               check(cudaMemcpyAsync(by.data(), g_.best_y, by.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") &&
+               check(cudaMemcpyAsync(dr.data(), g_.dray, dr.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") &&
+               check(cudaMemcpyAsync(pr.data(), g_.pray, pr.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") &&
+               check(cudaStreamSynchronize(stream_), "download");
+    }
+    out.clear();
+    for (size_t i = 0; i < spec_.lps.size(); ++i) {
+        const pdlpgpu_lp& lp = *spec_.lps[i];
+        auto* r = static_cast<pdlpgpu_result*>(std::calloc(1, sizeof(pdlpgpu_result)));
+        r->num_rows = lp.num_rows;
+        r->num_cols = lp.num_cols;
+        r->primal_objective = std::nan("");
+        r->dual_objective = -INFINITY;
+        r->primal_residual = r->dual_residual = r->relative_gap = INFINITY;
+        r->final_primal_weight = 1.0;
+        r->solve_time_seconds = elapsed;
+        const int b = device_of_[i];
+        if (b < 0) {
+            r->status = PDLPGPU_INVALID_PROBLEM;
+            std::snprintf(r->status_message, sizeof(r->status_message), "%s", invalid_[i].c_str());
+            out.push_back(r);
+            continue;
+        }
+        const InstanceCtl& c = ctl[static_cast<size_t>(b)];
+        if (!have || c.phase != kPhaseDone || c.status < 0) {
+            r->status = PDLPGPU_NUMERICAL_FAILURE;
+            std::snprintf(r->status_message, sizeof(r->status_message), "%s",
+                          error_.empty() ? "device loop did not complete" : error_.c_str());
+            out.push_back(r);
+            continue;
+        }
+        const MatrixLayout& L = layouts_[spec_.shared_matrix ? 0 : b];
+        const InstanceInfo& inf = info_[b];
+        r->status = c.status;
+        std::snprintf(r->status_message, sizeof(r->status_message), "%s", message_text(c.message));
+        r->primal = static_cast<double*>(std::malloc(sizeof(double) * std::max(1, lp.num_cols)));
+        r->row_dual = static_cast<double*>(std::malloc(sizeof(double) * std::max(1, lp.num_rows)));
+        for (int32_t k = 0; k < inf.n; ++k) r->primal[L.col_perm[k]] = bx[inf.col_off + k];
+        for (int32_t k = 0; k < inf.m; ++k) r->row_dual[L.row_perm[k]] = by[inf.row_off + k];
+        if (c.status == PDLPGPU_INFEASIBLE && c.ray_kind == 1) {
+            r->dual_ray = static_cast<double*>(std::malloc(sizeof(double) * std::max(1, lp.num_rows)));
+            for (int32_t k = 0; k < inf.m; ++k) r->dual_ray[L.row_perm[k]] = dr[inf.row_off + k];
+        }
+        if (c.status == PDLPGPU_UNBOUNDED && c.ray_kind == 2) {
+            r->primal_ray = static_cast<double*>(std::malloc(sizeof(double) * std::max(1, lp.num_cols)));
+            for (int32_t k = 0; k < inf.n; ++k) r->primal_ray[L.col_perm[k]] = pr[inf.col_off + k];
+        }
+        r->primal_objective = c.best_pobj;
+        r->dual_objective = c.best_dobj;
+        r->primal_residual = c.best_pres;
+        r->dual_residual = c.best_dres;
+        r->relative_gap = c.best_gap;
+        r->iterations = c.iteration;
+        r->step_trials = c.step_trials;
+        r->restart_count = c.restart_count;
+        if (c.diagnostics) {
+            r->final_step_size = c.eta;
+            r->static_step_bound = c.eta_max;
+            r->final_primal_weight = c.omega;
+        }
+        r->precision_used = mixed_ ? (c.fp64_stage ? 2 : 1) : 0;
+        r->fp64_iterations = c.fp64_iterations;
+        r->device_seconds = device_seconds_;
+        out.push_back(r);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Component tests
+// ---------------------------------------------------------------------------
+namespace {
+template <class T>
+std::vector<T> cast_vec(const std::vector<double>& v) {
+    return std::vector<T>(v.begin(), v.end());
+}
+}  // namespace
+
+bool Engine::component_spmv(int transpose, int values, const double* in, double* out) {
+    if (!setup_ok_ || count_ != 1) return false;
+    const int V = tuning_.vector_width;
+    launch_scale_values(g_, a_s64_, at_s64_, a_s32_, at_s32_, V, g_.a.num_ctas, g_.at.num_ctas, stream_);
+    std::vector<double> src;
+    if (transpose) to_internal_rows(in, src, 0); else to_internal_cols(in, src, 0);
+    const size_t out_n = transpose ? info_[0].n : info_[0].m;
+    std::vector<double> res(out_n);
+    if (values == 2) {
+        if (!mixed_) return false;
+        const std::vector<float> sf = cast_vec<float>(src);
+        float* din = transpose ? w32_.Y[0] : w32_.X[0];
+        float* dout = transpose ? w32_.X[1] : w32_.Y[1];
+        if (!check(cudaMemcpyAsync(din, sf.data(), sf.size() * 4, cudaMemcpyHostToDevice, stream_), "upload")) return false;
+        launch_spmv<float>(g_, transpose, 2, din, dout, V, stream_);
+        std::vector<float> rf(out_n);
+        if (!check(cudaMemcpyAsync(rf.data(), dout, out_n * 4, cudaMemcpyDeviceToHost, stream_), "download")) return false;
+        if (!check(cudaStreamSynchronize(stream_), "spmv")) return false;
+        for (size_t k = 0; k < out_n; ++k) res[k] = rf[k];
+    } else {
+        double* din = transpose ? g_.y_o : g_.x_o;
+        double* dout = transpose ? g_.x_o : g_.y_o;
+        if (!check(cudaMemcpyAsync(din, src.data(), src.size() * 8, cudaMemcpyHostToDevice, stream_), "upload")) return false;
+        launch_spmv<double>(g_, transpose, values, din, dout, V, stream_);
+        if (!check(cudaMemcpyAsync(res.data(), dout, out_n * 8, cudaMemcpyDeviceToHost, stream_), "download")) return false;
+        if (!check(cudaStreamSynchronize(stream_), "spmv")) return false;
+    }
+    const MatrixLayout& L = layouts_[0];
+    if (transpose) for (int32_t k = 0; k < L.n; ++k) out[L.col_perm[k]] = res[k];
+    else for (int32_t k = 0; k < L.m; ++k) out[L.row_perm[k]] = res[k];
+    return true;
+}
+
+bool Engine::component_ruiz(double* row_scale, double* col_scale, double* scaled_csr) {
+    if (!setup_ok_ || count_ != 1) return false;
+    const int V = tuning_.vector_width;
+    const pdlpgpu_options& o = spec_.opt;
+    for (int pass = 0; pass < o.ruiz_iterations; ++pass) {
+        launch_ruiz_max(g_, V, g_.a.num_ctas, g_.at.num_ctas, stream_);
+        launch_ruiz_update(g_, g_.num_vec, stream_);
+    }
+    launch_scale_values(g_, a_s64_, at_s64_, a_s32_, at_s32_, V, g_.a.num_ctas, g_.at.num_ctas, stream_);
+    const MatrixLayout& L = layouts_[0];
+    std::vector<double> rs(L.m), cs(L.n), slots(static_cast<size_t>(a_slots_));
+    if (!check(cudaMemcpyAsync(rs.data(), g_.rs, rs.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") ||
+        !check(cudaMemcpyAsync(cs.data(), g_.cs, cs.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") ||
+        !check(cudaMemcpyAsync(slots.data(), a_s64_, slots.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") ||
+        !check(cudaStreamSynchronize(stream_), "ruiz"))
+        return false;
+    for (int32_t k = 0; k < L.m; ++k) row_scale[L.row_perm[k]] = rs[k];
+    for (int32_t k = 0; k < L.n; ++k) col_scale[L.col_perm[k]] = cs[k];
+    if (scaled_csr != nullptr) {
+        const int Vw = tuning_.vector_width;
+        for (const SliceDesc& sd : L.a.slices) {
+            const int glog = slice_glog(sd.meta), nl = slice_lines(sd.meta), G = 1 << glog;
+            const int64_t base = static_cast<int64_t>(sd.data_off) * 32;
+            for (int r = 0; r < nl; ++r) {
+                const int32_t line = sd.line0 + r;
+                const int32_t row = L.row_perm[line];
+                for (int k = 0; k < L.a.line_len[line]; ++k) {
+                    const int64_t s = k >> glog;
+                    const int lane = r * G + (k & (G - 1));
+                    const int64_t pos = base + (s / Vw) * 32 * Vw + lane * Vw + (s % Vw);
+                    const int32_t col = L.col_perm[L.a.idx[pos]];
+                    const int32_t* b = csr0_.index.data() + csr0_.start[row];
+                    const int32_t* e = csr0_.index.data() + csr0_.start[row + 1];
+                    const int32_t* f = std::lower_bound(b, e, col);
+                    scaled_csr[f - csr0_.index.data()] = slots[pos];
+                }
+            }
+        }
+    }
+    return true;
+}
+
+bool Engine::component_precondition(double* tau, double* tau_inv, double* sigma, double* sigma_inv) {
+    if (!setup_ok_ || count_ != 1) return false;
+    const int V = tuning_.vector_width;
+    launch_scale_values(g_, a_s64_, at_s64_, a_s32_, at_s32_, V, g_.a.num_ctas, g_.at.num_ctas, stream_);
+    launch_precondition<double>(g_, w64_, 1, V, g_.a.num_ctas, g_.at.num_ctas, stream_);
+    const MatrixLayout& L = layouts_[0];
+    std::vector<double> t(L.n), ti(L.n), sg(L.m), si(L.m);
+    if (!check(cudaMemcpyAsync(t.data(), w64_.tau, t.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") ||
+        !check(cudaMemcpyAsync(ti.data(), w64_.itau, ti.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") ||
+        !check(cudaMemcpyAsync(sg.data(), w64_.sigma, sg.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") ||
+        !check(cudaMemcpyAsync(si.data(), w64_.isigma, si.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") ||
+        !check(cudaStreamSynchronize(stream_), "precondition"))
+        return false;
+    for (int32_t k = 0; k < L.n; ++k) { tau[L.col_perm[k]] = t[k]; tau_inv[L.col_perm[k]] = ti[k]; }
+    for (int32_t k = 0; k < L.m; ++k) { sigma[L.row_perm[k]] = sg[k]; sigma_inv[L.row_perm[k]] = si[k]; }
+    return true;
+}
+
+namespace {
+template <class T>
+bool put(cudaStream_t s, T* dst, const std::vector<double>& src) {
+    const std::vector<T> v(src.begin(), src.end());
+    return cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s) == cudaSuccess;
+}
+template <class T>
+bool get(cudaStream_t s, const T* src, std::vector<double>& dst, size_t n) {
+    std::vector<T> v(n);
+    if (cudaMemcpyAsync(v.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost, s) != cudaSuccess) return false;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return false;
+    dst.assign(v.begin(), v.end());
+    return true;
+}
+}  // namespace
+
+bool Engine::component_trial(const double* tau, const double* tau_inv, const double* sigma,
+                             const double* sigma_inv, const double* x, const double* y,
+                             const double* ax, double step, double weight, double* x_out,
+                             double* y_out, double* ax_out, double* reductions) {
+    if (!setup_ok_ || count_ != 1) return false;
+    const int V = tuning_.vector_width;
+    launch_scale_values(g_, a_s64_, at_s64_, a_s32_, at_s32_, V, g_.a.num_ctas, g_.at.num_ctas, stream_);
+    launch_setup_vectors<double>(g_, w64_, stream_);
+    if (mixed_) launch_setup_vectors<float>(g_, w32_, stream_);
+    std::vector<double> t, ti, sg, si, xv, yv, av;
+    to_internal_cols(tau, t, 0);
+    to_internal_cols(tau_inv, ti, 0);
+    to_internal_rows(sigma, sg, 0);
+    to_internal_rows(sigma_inv, si, 0);
+    to_internal_cols(x, xv, 0);
+    to_internal_rows(y, yv, 0);
+    to_internal_rows(ax, av, 0);
+    InstanceCtl c;
+    std::memset(&c, 0, sizeof(c));
+    c.phase = kPhaseMain;
+    c.stage = kStageTrial;
+    c.fp64_stage = mixed_ ? 0 : 1;
+    c.eta = c.trial_eta = step;
+    c.omega = c.trial_omega = weight;
+    c.eta_max = 1.0;
+    c.best_kkt = INFINITY;
+    bool ok = check(cudaMemcpyAsync(g_.ctl, &c, sizeof(c), cudaMemcpyHostToDevice, stream_), "upload");
+    std::vector<double> xo, yo, ao;
+    const MatrixLayout& L = layouts_[0];
+    if (mixed_) {
+        ok = ok && put(stream_, w32_.tau, t) && put(stream_, w32_.itau, ti) && put(stream_, w32_.sigma, sg) &&
+             put(stream_, w32_.isigma, si) && put(stream_, w32_.X[0], xv) && put(stream_, w32_.Y[0], yv) &&
+             put(stream_, w32_.AX[0], av);
+        if (!ok) return check(cudaErrorInvalidValue, "upload");
+        launch_primal<float>(g_, w32_, dopt_, V, stream_);
+        launch_dual<float>(g_, w32_, dopt_, V, stream_);
+        ok = get(stream_, w32_.X[1], xo, L.n) && get(stream_, w32_.Y[1], yo, L.m) && get(stream_, w32_.AX[1], ao, L.m);
+    } else {
+        ok = ok && put(stream_, w64_.tau, t) && put(stream_, w64_.itau, ti) && put(stream_, w64_.sigma, sg) &&
+             put(stream_, w64_.isigma, si) && put(stream_, w64_.X[0], xv) && put(stream_, w64_.Y[0], yv) &&
+             put(stream_, w64_.AX[0], av);
+        if (!ok) return check(cudaErrorInvalidValue, "upload");
+        launch_primal<double>(g_, w64_, dopt_, V, stream_);
+        launch_dual<double>(g_, w64_, dopt_, V, stream_);
+        ok = get(stream_, w64_.X[1], xo, L.n) && get(stream_, w64_.Y[1], yo, L.m) && get(stream_, w64_.AX[1], ao, L.m);
+    }
+    if (!ok || !check(cudaGetLastError(), "trial")) return false;
+    if (!check(cudaMemcpyAsync(&c, g_.ctl, sizeof(c), cudaMemcpyDeviceToHost, stream_), "download") ||
+        !check(cudaStreamSynchronize(stream_), "trial"))
+        return false;
+    for (int32_t k = 0; k < L.n; ++k) x_out[L.col_perm[k]] = xo[k];
+    for (int32_t k = 0; k < L.m; ++k) { y_out[L.row_perm[k]] = yo[k]; ax_out[L.row_perm[k]] = ao[k]; }
+    reductions[0] = c.dbg[0];
+    reductions[1] = c.dbg[1];
+    reductions[2] = c.dbg[2];
+    return true;
+}
+
+bool Engine::component_evaluate(const double* x, const double* y, const double* rx,
+                                const double* ry, double* metrics, double* verdicts) {
+    if (!setup_ok_ || count_ != 1) return false;
+    const int V = tuning_.vector_width;
+    launch_scale_values(g_, a_s64_, at_s64_, a_s32_, at_s32_, V, g_.a.num_ctas, g_.at.num_ctas, stream_);
+    launch_setup_vectors<double>(g_, w64_, stream_);
+    std::vector<double> xv, yv, rxv, ryv;
+    to_internal_cols(x, xv, 0);
+    to_internal_rows(y, yv, 0);
+    to_internal_cols(rx, rxv, 0);
+    to_internal_rows(ry, ryv, 0);
+    InstanceCtl c;
+    std::memset(&c, 0, sizeof(c));
+    c.phase = kPhaseMain;
+    c.stage = kStageCheck;
+    c.check_kind = kCheckEvaluate;
+    c.fp64_stage = 1;
+    normalisers(*spec_.lps[0], c.pnorm, c.dnorm);
+    c.objective_offset = spec_.lps[0]->objective_offset;
+    c.best_kkt = INFINITY;
+    bool ok = check(cudaMemcpyAsync(g_.ctl, &c, sizeof(c), cudaMemcpyHostToDevice, stream_), "upload") &&
+              put(stream_, w64_.X[0], xv) && put(stream_, w64_.Y[0], yv) && put(stream_, w64_.rx, rxv) &&
+              put(stream_, w64_.ry, ryv);
+    if (!ok) return check(cudaErrorInvalidValue, "upload");
+    launch_check_prep<double>(g_, w64_, dopt_, stream_);
+    launch_check_spmv(g_, dopt_, V, stream_);
+    if (!check(cudaMemcpyAsync(&c, g_.ctl, sizeof(c), cudaMemcpyDeviceToHost, stream_), "download") ||
+        !check(cudaStreamSynchronize(stream_), "evaluate"))
+        return false;
+    metrics[0] = c.best_pobj;
+    metrics[1] = c.best_dobj;
+    metrics[2] = c.best_pres;
+    metrics[3] = c.best_dres;
+    metrics[4] = c.best_gap;
+    metrics[5] = c.best_kkt;
+    metrics[6] = c.best_finite;
+    metrics[7] = c.best_valid;
+    for (int q = 0; q < 6; ++q) verdicts[q] = c.dbg[3 + q];
+    return true;
+}
+
+}  // namespace pdlpgpu

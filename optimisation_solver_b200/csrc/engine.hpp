@@ -1,0 +1,120 @@
+// engine.hpp -- host side of the device PDLP engine.
+#pragma once
+
+#include "kernels.cuh"
+#include "layout.hpp"
+#include "pdlpgpu.h"
+
+#include <chrono>
+#include <string>
+#include <vector>
+
+namespace pdlpgpu {
+
+struct SolveSpec {
+    std::vector<const pdlpgpu_lp*> lps;   // one per instance
+    bool shared_matrix = false;           // every instance uses lps[0]'s matrix
+    pdlpgpu_options opt{};
+    pdlpgpu_ext_options ext{};
+    std::vector<const pdlpgpu_warmstart*> warm;   // empty or one (nullable) per instance
+    // Component tests: the LP is used as the working problem (no Ruiz pass),
+    // and the caller may supply the preconditioner.
+    bool working_given = false;
+    const double* given_tau = nullptr;
+    const double* given_sigma = nullptr;
+};
+
+// Device-side arrays of one batch. All live in one allocation.
+class Engine {
+public:
+    explicit Engine(int device);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    // Host validation, layout and upload (prepare), then control state, the
+    // setup kernels and the initial check (start). Returns false on a setup
+    // failure (error()); invalid instances are recorded per instance.
+    bool prepare(const SolveSpec& spec);
+    bool start();
+    bool setup(const SolveSpec& spec) { return prepare(spec) && start(); }
+    // The iteration loop, to completion of every instance.
+    bool run();
+    // One result per instance of the spec (invalid ones included).
+    void results(std::vector<pdlpgpu_result*>& out);
+
+    const std::string& error() const { return error_; }
+    double device_seconds() const { return device_seconds_; }
+    int64_t launches() const { return launches_; }
+
+    // --- component tests (single instance, internal order handled here) ---
+    bool component_spmv(int transpose, int values, const double* in, double* out);
+    bool component_ruiz(double* row_scale, double* col_scale, double* scaled_csr);
+    bool component_precondition(double* tau, double* tau_inv, double* sigma, double* sigma_inv);
+    bool component_trial(const double* tau, const double* tau_inv, const double* sigma,
+                         const double* sigma_inv, const double* x, const double* y,
+                         const double* ax, double step, double weight, double* x_out,
+                         double* y_out, double* ax_out, double* reductions);
+    bool component_evaluate(const double* x, const double* y, const double* rx, const double* ry,
+                            double* metrics, double* verdicts);
+
+private:
+    template <class T> void enqueue_trial(const Work<T>& w);
+    template <class T> void enqueue_check(const Work<T>& w);
+    void enqueue_chunk(int slots);
+    void enqueue_check_stage();
+    bool check(cudaError_t e, const char* what);
+    bool build_graph(int slots);
+    bool power_iteration();
+    bool setup_kernels();
+    bool init_control();
+    template <class V> void to_internal_cols(const V* src, std::vector<V>& dst, int instance) const;
+    template <class V> void to_internal_rows(const V* src, std::vector<V>& dst, int instance) const;
+
+    int device_ = 0;
+    int sms_ = 148;
+    cudaStream_t stream_ = nullptr;
+    cudaGraphExec_t graph_ = nullptr;
+    int graph_slots_ = 0;
+    char* arena_ = nullptr;
+    size_t arena_bytes_ = 0;
+    std::string error_;
+    std::chrono::steady_clock::time_point t0_;
+
+    // spec-derived
+    SolveSpec spec_;
+    bool mixed_ = false;
+    Tuning tuning_;
+    int32_t count_ = 0;                  // device instances
+    std::vector<int32_t> device_of_;     // spec instance -> device instance or -1
+    std::vector<std::string> invalid_;   // per spec instance: message if invalid
+    std::vector<MatrixLayout> layouts_;  // per device instance (one when shared)
+    std::vector<InstanceInfo> info_;
+    int64_t rows_total_ = 0, cols_total_ = 0;
+    int64_t a_slots_ = 0, at_slots_ = 0;
+    int32_t a_slices_ = 0, at_slices_ = 0;
+    std::vector<CtaWork> a_ctas_, at_ctas_;
+    std::vector<VecWork> vec_;
+    int first_a_ctas_ = 0, first_at_ctas_ = 0, first_vec_ = 0;
+    HostCsr csr0_;                       // canonical A of instance 0 (component tests)
+
+    // device
+    Global g_{};
+    Work<double> w64_{};
+    Work<float> w32_{};
+    DeviceOptions dopt_{};
+    double* a_s64_ = nullptr;
+    double* at_s64_ = nullptr;
+    float* a_s32_ = nullptr;
+    float* at_s32_ = nullptr;
+    int32_t* d_active_ = nullptr;
+    int32_t* h_active_ = nullptr;     // pinned
+    double device_seconds_ = 0.0;
+    int64_t launches_ = 0;
+    bool ran_ = false;
+    bool setup_ok_ = false;
+};
+
+const char* message_text(int32_t id);
+
+}  // namespace pdlpgpu

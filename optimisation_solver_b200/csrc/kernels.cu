@@ -1,0 +1,1308 @@
+// kernels.cu -- the device kernels of the PDLP engine (sm_100a).
+//
+// Hot path, per linesearch trial (pdlp_engine/src/pdhg_kernel.cpp:47-277):
+//   k_primal  over the A^T side: g = c + A'y, x' = clip(x - (eta/omega) tau g),
+//             sum dx^2/tau; applies the iterate-average update owed by the last
+//             commit (iterate_average.cpp:40-82) while x is in registers.
+//   k_dual    over the A side: A x', extrapolation 2Ax' - Ax, dual prox
+//             y' = max(v - s u, 0) + min(v - s l, 0), sum dy^2/sigma and
+//             dy'(A dx); owed average update of y; then, in the last CTA of each
+//             instance, the linesearch decision and commit (trial_control).
+// Every check_frequency iterations (termination.cpp:66-325,
+// infeasibility.cpp:51-192, pdlp_solver.cpp:354-476), in FP64 on the original
+// problem:
+//   k_check_prep   elementwise: original-coordinate copies of the current and
+//                  averaged iterates and of the ray directions, and every
+//                  reduction that needs no matrix product
+//   k_check_spmv   both matrix passes at once, each gathering up to three
+//                  vectors; the last CTA of an instance decides (best point,
+//                  certificates, termination, restart)
+//   k_check_apply  best-point copies, restarts, polishing entry, ray copies
+//   k_refresh      A x after an iterate was replaced
+//   k_finalize     clears the per-check flags
+// Setup: Ruiz max-abs passes, scaled coefficients, Pock-Chambolle sums.
+//
+// Gathers go through the read-only path; matrix streams use 128-bit loads
+// when the vector width allows. No atomics touch numerical data: the only
+// atomic is the per-instance arrival counter.
+#include "control.cuh"
+#include "kernels.cuh"
+
+#include <cstdio>
+
+namespace pdlpgpu {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// ---------------------------------------------------------------------------
+// Loads of V consecutive elements (V in {1, 2, 4}); the caller guarantees
+// V-element alignment.
+// ---------------------------------------------------------------------------
+template <int V> __device__ __forceinline__ void ld(const int32_t* p, int32_t (&o)[V]);
+template <> __device__ __forceinline__ void ld<1>(const int32_t* p, int32_t (&o)[1]) { o[0] = __ldg(p); }
+template <> __device__ __forceinline__ void ld<2>(const int32_t* p, int32_t (&o)[2]) {
+    const int2 v = __ldg(reinterpret_cast<const int2*>(p)); o[0] = v.x; o[1] = v.y;
+}
+template <> __device__ __forceinline__ void ld<4>(const int32_t* p, int32_t (&o)[4]) {
+    const int4 v = __ldg(reinterpret_cast<const int4*>(p)); o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+template <int V> __device__ __forceinline__ void ld(const float* p, float (&o)[V]);
+template <> __device__ __forceinline__ void ld<1>(const float* p, float (&o)[1]) { o[0] = __ldg(p); }
+template <> __device__ __forceinline__ void ld<2>(const float* p, float (&o)[2]) {
+    const float2 v = __ldg(reinterpret_cast<const float2*>(p)); o[0] = v.x; o[1] = v.y;
+}
+template <> __device__ __forceinline__ void ld<4>(const float* p, float (&o)[4]) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p)); o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+template <int V> __device__ __forceinline__ void ld(const double* p, double (&o)[V]);
+template <> __device__ __forceinline__ void ld<1>(const double* p, double (&o)[1]) { o[0] = __ldg(p); }
+template <> __device__ __forceinline__ void ld<2>(const double* p, double (&o)[2]) {
+    const double2 v = __ldg(reinterpret_cast<const double2*>(p)); o[0] = v.x; o[1] = v.y;
+}
+template <> __device__ __forceinline__ void ld<4>(const double* p, double (&o)[4]) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p + 2));
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+
+// Lane position inside a slice.
+struct LanePos {
+    int glog;     // log2 of the lane group
+    int g;        // lane inside the group
+    int line;     // local line index
+    bool valid;   // the lane's line exists
+};
+
+__device__ __forceinline__ LanePos lane_pos(const SliceDesc& sd, int lane) {
+    LanePos p;
+    p.glog = slice_glog(sd.meta);
+    const int r = lane >> p.glog;
+    p.g = lane & ((1 << p.glog) - 1);
+    p.line = sd.line0 + r;
+    p.valid = r < slice_lines(sd.meta);
+    return p;
+}
+
+// Sum of NQ products over the lane's entries of one line, then combined over
+// the G lanes of the line with an xor butterfly (every lane ends with the same
+// bits, so the result is deterministic).
+template <int V, int NQ, class TA, class TV, class F>
+__device__ __forceinline__ void line_sums(int64_t base, int steps, const LanePos& lp, int lane,
+                                          int len, const int32_t* __restrict__ idx,
+                                          const TV* __restrict__ val, TA (&acc)[NQ], F fetch) {
+#pragma unroll 2
+    for (int s = 0; s < steps; s += V) {
+        const int64_t p = base + static_cast<int64_t>(s) * 32 + lane * V;
+        int32_t id[V];
+        TV v[V];
+        ld<V>(idx + p, id);
+        ld<V>(val + p, v);
+#pragma unroll
+        for (int q = 0; q < V; ++q) {
+            const int k = ((s + q) << lp.glog) + lp.g;
+            if (k < len) fetch(acc, static_cast<TA>(v[q]), id[q]);
+        }
+    }
+    for (int o = (1 << lp.glog) >> 1; o > 0; o >>= 1) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) acc[q] += __shfl_xor_sync(kFull, acc[q], o);
+    }
+}
+
+// Block-wide deterministic sum of NQ doubles; the result is valid in thread 0.
+template <int NQ>
+__device__ __forceinline__ void block_sum(double (&v)[NQ]) {
+    __shared__ double red[NQ][kWarps * 4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(kFull, v[q], o);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) red[q][warp] = v[q];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double t = 0.0;
+            for (int w = 0; w < warps; ++w) t += red[q][w];
+            v[q] = t;
+        }
+    }
+}
+
+// Warp-0 deterministic sum over a range of per-CTA partials (stride `slots`).
+__device__ __forceinline__ double warp_range_sum(const double* part, int begin, int end,
+                                                 int slots, int slot) {
+    const int lane = threadIdx.x & 31;
+    double t = 0.0;
+    for (int k = begin + lane; k < end; k += 32) t += part[static_cast<int64_t>(k) * slots + slot];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kFull, t, o);
+    return t;
+}
+
+// Arrival counter: returns true in every thread of the CTA that arrives last
+// among `expected` CTAs of the instance (and resets the counter for the next
+// launch). Partials written before the call are visible to that CTA.
+__device__ __forceinline__ bool arrive_last(int32_t* counter, int expected) {
+    __shared__ int last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int prev = atomicAdd(counter, 1);
+        last = prev == expected - 1;
+        if (last) *counter = 0;
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last != 0;
+}
+
+template <class T>
+__device__ __forceinline__ bool precision_matches(const InstanceCtl& c) {
+    return (c.fp64_stage != 0) == (sizeof(T) == 8);
+}
+
+template <class T>
+__device__ __forceinline__ bool trial_active(const InstanceCtl& c) {
+    return c.phase != kPhaseDone && c.stage == kStageTrial && precision_matches<T>(c);
+}
+
+__device__ __forceinline__ bool check_have_avg(const InstanceCtl& c, const DeviceOptions& o) {
+    if (c.check_kind == kCheckInitial) return c.have_avg_at_check != 0;
+    return o.averaging && c.avg_weight != 0.0;
+}
+
+template <class T> __device__ __forceinline__ const T* matrix_values(const Side& s);
+template <> __device__ __forceinline__ const double* matrix_values<double>(const Side& s) { return s.val_s64; }
+template <> __device__ __forceinline__ const float* matrix_values<float>(const Side& s) { return s.val_s32; }
+
+template <class T> __device__ __forceinline__ T min_dual_step();
+template <> __device__ __forceinline__ double min_dual_step<double>() { return 1e-300; }
+template <> __device__ __forceinline__ float min_dual_step<float>() { return 1e-37f; }
+
+// ---------------------------------------------------------------------------
+// Primal half (pdhg_kernel.cpp:47-104)
+// ---------------------------------------------------------------------------
+template <class T, int V>
+__global__ void __launch_bounds__(kThreads) k_primal(Global g, Work<T> w) {
+    const CtaWork cw = g.at.ctas[blockIdx.x];
+    const InstanceCtl& c = g.ctl[cw.instance];
+    if (!trial_active<T>(c)) return;
+    const InstanceInfo inf = g.info[cw.instance];
+    const int p = c.parity;
+    const T mult = static_cast<T>(c.trial_eta / c.trial_omega);
+    const bool pending = c.pending_avg != 0;
+    const T frac = static_cast<T>(c.avg_frac);
+
+    const T* __restrict__ y = w.Y[p] + inf.row_off;
+    const T* __restrict__ x = w.X[p] + inf.col_off;
+    T* __restrict__ xt = w.X[p ^ 1] + inf.col_off;
+    const T* __restrict__ cv = w.c + inf.col_off;
+    const T* __restrict__ lo = w.xl + inf.col_off;
+    const T* __restrict__ hi = w.xu + inf.col_off;
+    const T* __restrict__ tau = w.tau + inf.col_off;
+    const T* __restrict__ itau = w.itau + inf.col_off;
+    T* __restrict__ avg = w.avg_x + inf.col_off;
+    const T* vals = matrix_values<T>(g.at);
+
+    double moved[1] = {0.0};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int s = cw.slice_begin + warp; s < cw.slice_end; s += kWarps) {
+        const SliceDesc sd = g.at.slices[s];
+        const LanePos lp = lane_pos(sd, lane);
+        const int len = lp.valid ? g.at.line_len[inf.at_len_base + lp.line] : 0;
+        T sum[1] = {T(0)};
+        line_sums<V, 1>(inf.at_data_base + static_cast<int64_t>(sd.data_off) * 32, sd.steps, lp,
+                        lane, len, g.at.idx, vals, sum,
+                        [&](T (&a)[1], T v, int i) { a[0] += v * y[i]; });
+        if (lp.valid && lp.g == 0) {
+            const int j = lp.line;
+            const T gradient = cv[j] + sum[0];
+            const T prev = x[j];
+            const T upd = smax(lo[j], smin(prev - mult * tau[j] * gradient, hi[j]));
+            xt[j] = upd;
+            const double d = static_cast<double>(upd - prev);
+            moved[0] += d * d * static_cast<double>(itau[j]);
+            if (pending) {
+                const T a = avg[j];
+                avg[j] = a + frac * (prev - a);
+            }
+        }
+    }
+    block_sum<1>(moved);
+    if (threadIdx.x == 0) g.part_primal[blockIdx.x] = moved[0];
+}
+
+// ---------------------------------------------------------------------------
+// Dual half (pdhg_kernel.cpp:109-187) and the trial decision
+// ---------------------------------------------------------------------------
+template <class T, int V>
+__global__ void __launch_bounds__(kThreads) k_dual(Global g, Work<T> w, DeviceOptions o) {
+    const CtaWork cw = g.a.ctas[blockIdx.x];
+    InstanceCtl& c = g.ctl[cw.instance];
+    if (!trial_active<T>(c)) return;
+    const InstanceInfo inf = g.info[cw.instance];
+    const int p = c.parity;
+    const T dm = static_cast<T>(c.trial_eta * c.trial_omega);
+    const bool pending = c.pending_avg != 0;
+    const T frac = static_cast<T>(c.avg_frac);
+
+    const T* __restrict__ xt = w.X[p ^ 1] + inf.col_off;
+    const T* __restrict__ y = w.Y[p] + inf.row_off;
+    T* __restrict__ yt = w.Y[p ^ 1] + inf.row_off;
+    const T* __restrict__ ax = w.AX[p] + inf.row_off;
+    T* __restrict__ axt = w.AX[p ^ 1] + inf.row_off;
+    const T* __restrict__ lo = w.rl + inf.row_off;
+    const T* __restrict__ hi = w.ru + inf.row_off;
+    const T* __restrict__ sig = w.sigma + inf.row_off;
+    const T* __restrict__ isig = w.isigma + inf.row_off;
+    T* __restrict__ avg = w.avg_y + inf.row_off;
+    const T* vals = matrix_values<T>(g.a);
+
+    double red[2] = {0.0, 0.0};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int s = cw.slice_begin + warp; s < cw.slice_end; s += kWarps) {
+        const SliceDesc sd = g.a.slices[s];
+        const LanePos lp = lane_pos(sd, lane);
+        const int len = lp.valid ? g.a.line_len[inf.a_len_base + lp.line] : 0;
+        T sum[1] = {T(0)};
+        line_sums<V, 1>(inf.a_data_base + static_cast<int64_t>(sd.data_off) * 32, sd.steps, lp,
+                        lane, len, g.a.idx, vals, sum,
+                        [&](T (&a)[1], T v, int j) { a[0] += v * xt[j]; });
+        if (lp.valid && lp.g == 0) {
+            const int i = lp.line;
+            const T next = sum[0];
+            const T dact = next - ax[i];
+            const T ext = next + dact;
+            const T step = smax(dm * sig[i], min_dual_step<T>());
+            const T prev = y[i];
+            const T v = prev + step * ext;
+            const T upd = smax(v - step * hi[i], T(0)) + smin(v - step * lo[i], T(0));
+            yt[i] = upd;
+            axt[i] = next;
+            const double d = static_cast<double>(upd - prev);
+            red[0] += d * d * static_cast<double>(isig[i]);
+            red[1] += d * static_cast<double>(dact);
+            if (pending) {
+                const T a = avg[i];
+                avg[i] = a + frac * (prev - a);
+            }
+        }
+    }
+    block_sum<2>(red);
+    if (threadIdx.x == 0) {
+        g.part_dual[2 * blockIdx.x] = red[0];
+        g.part_dual[2 * blockIdx.x + 1] = red[1];
+    }
+    if (!arrive_last(g.count_dual + cw.instance, inf.a_cta_end - inf.a_cta_begin)) return;
+    if (threadIdx.x < 32) {
+        const double pm = warp_range_sum(g.part_primal, inf.at_cta_begin, inf.at_cta_end, 1, 0);
+        const double dmv = warp_range_sum(g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 0);
+        const double it = warp_range_sum(g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 1);
+        if (threadIdx.x == 0) trial_control(c, o, pm, dmv, it, inf.n);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Check, elementwise part (termination.cpp rowPass/columnPass terms without a
+// product, infeasibility.cpp normalisation and cone projections,
+// pdlp_solver.cpp:373-389 and :455-459)
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_check_prep(Global g, Work<T> w, DeviceOptions o) {
+    const VecWork vw = g.vec[blockIdx.x];
+    const InstanceCtl& c = g.ctl[vw.instance];
+    if (c.stage != kStageCheck || c.check_kind == kCheckTransition || !precision_matches<T>(c)) return;
+    const InstanceInfo inf = g.info[vw.instance];
+    const int p = c.parity;
+    const bool pending = c.pending_avg != 0;
+    const T frac = static_cast<T>(c.avg_frac);
+    const bool have_avg = check_have_avg(c, o);
+    const bool rays =
+        (c.check_kind == kCheckMain || c.check_kind == kCheckEvaluate) && o.detect_infeasibility;
+
+    double acc[kPrepSlots];
+#pragma unroll
+    for (int q = 0; q < kPrepSlots; ++q) acc[q] = 0.0;
+
+    if (!vw.is_row) {
+        const int64_t off = inf.col_off;
+        for (int j = vw.begin + threadIdx.x; j < vw.end; j += blockDim.x) {
+            const int64_t k = off + j;
+            const T x = w.X[p][k];
+            T a = w.avg_x[k];
+            if (pending) {
+                a = a + frac * (x - a);
+                w.avg_x[k] = a;
+            }
+            const double cs = g.cs[k];
+            const double xo = cs * static_cast<double>(x);
+            g.x_o[k] = xo;
+            const double co = g.c_orig[k];
+            acc[0] += co * xo;
+            if (have_avg) {
+                const double xao = cs * static_cast<double>(a);
+                g.xa_o[k] = xao;
+                acc[1] += co * xao;
+            }
+            if (rays) {
+                const double d = cs * (static_cast<double>(x) - static_cast<double>(w.rx[k]));
+                acc[2] += d * d;
+                double q = d;
+                if (isfinite(g.xu_orig[k])) q = smin(q, 0.0);
+                if (isfinite(g.xl_orig[k])) q = smax(q, 0.0);
+                const double drift = d - q;
+                acc[3] += drift * drift;
+                acc[4] += co * q;
+                g.p_proj[k] = q;
+            }
+            if (c.check_kind == kCheckMain) {
+                const double r = static_cast<double>(w.rx[k]);
+                const double dc = static_cast<double>(x) - r;
+                acc[5] += dc * dc;
+                const double da = static_cast<double>(a) - r;
+                acc[6] += da * da;
+            }
+        }
+    } else {
+        const int64_t off = inf.row_off;
+        for (int i = vw.begin + threadIdx.x; i < vw.end; i += blockDim.x) {
+            const int64_t k = off + i;
+            const T y = w.Y[p][k];
+            T a = w.avg_y[k];
+            if (pending) {
+                a = a + frac * (y - a);
+                w.avg_y[k] = a;
+            }
+            const double rs = g.rs[k];
+            const double lo = g.rl_orig[k], hi = g.ru_orig[k];
+            const bool lo_f = isfinite(lo), hi_f = isfinite(hi);
+            const double yo = rs * static_cast<double>(y);
+            g.y_o[k] = yo;
+            {
+                double q = yo;
+                if (!hi_f) q = smin(q, 0.0);
+                if (!lo_f) q = smax(q, 0.0);
+                const double drift = yo - q;
+                acc[1] += drift * drift;
+                if (q > 0.0) acc[0] += q * hi;
+                else if (q < 0.0) acc[0] += q * lo;
+            }
+            if (have_avg) {
+                const double yao = rs * static_cast<double>(a);
+                g.ya_o[k] = yao;
+                double q = yao;
+                if (!hi_f) q = smin(q, 0.0);
+                if (!lo_f) q = smax(q, 0.0);
+                const double drift = yao - q;
+                acc[3] += drift * drift;
+                if (q > 0.0) acc[2] += q * hi;
+                else if (q < 0.0) acc[2] += q * lo;
+            }
+            if (rays) {
+                const double d = rs * (static_cast<double>(y) - static_cast<double>(w.ry[k]));
+                g.dy_o[k] = d;
+                acc[4] += d * d;
+                double q = d;
+                if (!hi_f) q = smin(q, 0.0);
+                if (!lo_f) q = smax(q, 0.0);
+                const double drift = d - q;
+                acc[5] += drift * drift;
+                if (q > 0.0) acc[6] += q * hi;
+                else if (q < 0.0) acc[6] += q * lo;
+            }
+            if (c.check_kind == kCheckMain) {
+                const double r = static_cast<double>(w.ry[k]);
+                const double dc = static_cast<double>(y) - r;
+                acc[7] += dc * dc;
+                const double da = static_cast<double>(a) - r;
+                acc[8] += da * da;
+            }
+        }
+    }
+    block_sum<kPrepSlots>(acc);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < kPrepSlots; ++q)
+            g.part_prep[static_cast<int64_t>(blockIdx.x) * kPrepSlots + q] = acc[q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Check, matrix passes and decision
+// ---------------------------------------------------------------------------
+__device__ void check_control(const Global& g, const DeviceOptions& o, InstanceCtl& c,
+                              const InstanceInfo& inf) {
+    // Column-side and row-side elementwise partials.
+    double C[kPrepSlots], R[kPrepSlots], A3[3], T6[kCheckSlots];
+    for (int q = 0; q < kPrepSlots; ++q) { C[q] = 0.0; R[q] = 0.0; }
+    const int lane = threadIdx.x & 31;
+    for (int q = 0; q < kPrepSlots; ++q) {
+        double tc = 0.0, tr = 0.0;
+        for (int k = inf.vec_cta_begin + lane; k < inf.vec_cta_end; k += 32) {
+            const double v = g.part_prep[static_cast<int64_t>(k) * kPrepSlots + q];
+            if (g.vec[k].is_row) tr += v; else tc += v;
+        }
+        for (int s = 16; s > 0; s >>= 1) {
+            tc += __shfl_xor_sync(kFull, tc, s);
+            tr += __shfl_xor_sync(kFull, tr, s);
+        }
+        C[q] = tc;
+        R[q] = tr;
+    }
+    for (int q = 0; q < 3; ++q)
+        A3[q] = warp_range_sum(g.part_check, inf.a_cta_begin, inf.a_cta_end, kCheckSlots, q);
+    const int at0 = g.a.num_ctas + inf.at_cta_begin, at1 = g.a.num_ctas + inf.at_cta_end;
+    for (int q = 0; q < kCheckSlots; ++q) T6[q] = warp_range_sum(g.part_check, at0, at1, kCheckSlots, q);
+    if (lane != 0) return;
+
+    c.pending_avg = 0;
+    const bool have_avg = check_have_avg(c, o);
+    const Metrics cur = make_metrics(c, A3[0], R[0], R[1], C[0], T6[1], T6[0]);
+    const Metrics avg = have_avg ? make_metrics(c, A3[1], R[2], R[3], C[1], T6[3], T6[2]) : cur;
+
+    if (c.check_kind == kCheckEvaluate) {
+        store_best(c, cur);
+        for (int q = 3; q < 12; ++q) c.dbg[q] = 0.0;
+        const double dn = sqrt(R[4]);
+        if (o.detect_infeasibility && dn > 1e-300 && isfinite(dn)) {
+            const double inv = 1.0 / dn;
+            const double value = (T6[5] - R[6]) * inv;
+            c.dbg[4] = value;
+            c.dbg[5] = 1.0;
+            if (isfinite(value) && value > 0.0) {
+                c.dbg[5] = sqrt(T6[4] + R[5]) * inv / value;
+                c.dbg[3] = c.dbg[5] <= o.infeasibility_tol ? 1.0 : 0.0;
+            }
+        }
+        const double pn = sqrt(C[2]);
+        if (o.detect_infeasibility && pn > 1e-300 && isfinite(pn)) {
+            const double inv = 1.0 / pn;
+            const double rate = C[4] * inv;
+            c.dbg[7] = rate;
+            c.dbg[8] = 1.0;
+            if (isfinite(rate) && rate < 0.0) {
+                c.dbg[8] = sqrt(C[3] + A3[2]) * inv / (-rate);
+                c.dbg[6] = c.dbg[8] <= o.infeasibility_tol ? 1.0 : 0.0;
+            }
+        }
+        c.stage = kStageTrial;
+        c.phase = kPhaseDone;
+        return;
+    }
+
+    if (c.check_kind == kCheckInitial) {
+        // pdlp_solver.cpp:239-264 (a warm start competes with the cold point,
+        // which sits in the average buffers).
+        c.restart_src = 1;
+        Metrics start = cur;
+        c.best_src = 1;
+        if (have_avg && avg.kkt < cur.kkt) {
+            start = avg;
+            c.best_src = 2;
+            c.restart_src = 2;
+            c.need_refresh = 1;
+        }
+        store_best(c, start);
+        c.restart_baseline = start.kkt;
+        c.avg_weight = 0.0;
+        c.have_avg_at_check = 0;
+        if (is_optimal_best(c, o)) {
+            finish(c, 0, kMsgInitialOptimal, false);
+            return;
+        }
+        loop_top_main(c, o, inf.n);
+        return;
+    }
+
+    if (c.check_kind == kCheckPolish) {   // feasibility_polishing.cpp:107-141
+        if (c.polish_deadline_ns > 0 && now_ns() >= c.polish_deadline_ns) {
+            end_polish(c, o);
+            return;
+        }
+        if (cur.kkt < c.best_kkt) {
+            c.best_src = 1;
+            store_best(c, cur);
+        }
+        if (have_avg && avg.kkt < c.best_kkt) {
+            c.best_src = 2;
+            store_best(c, avg);
+        }
+        if (is_optimal_best(c, o) || c.polish_done_iterations == o.polishing_iterations) {
+            end_polish(c, o);
+            return;
+        }
+        c.stage = kStageTrial;
+        return;
+    }
+
+    // Main check (pdlp_solver.cpp:354-476).
+    if (cur.kkt < c.best_kkt) {
+        c.best_src = 1;
+        store_best(c, cur);
+    }
+    if (have_avg && avg.kkt < c.best_kkt) {
+        c.best_src = 2;
+        store_best(c, avg);
+    }
+    if (o.detect_infeasibility) {
+        // Dual ray: value = inf_box (A'd)'x - support(d), both linear in d, so
+        // the sums over the raw direction are scaled by 1/||d|| afterwards.
+        const double dn = sqrt(R[4]);
+        if (dn > 1e-300 && isfinite(dn)) {
+            const double inv = 1.0 / dn;
+            const double value = (T6[5] - R[6]) * inv;
+            if (isfinite(value) && value > 0.0) {
+                const double viol = sqrt(T6[4] + R[5]) * inv;
+                if (viol / value <= o.infeasibility_tol) {
+                    finish(c, 1, kMsgInfeasible, true);
+                    c.save_ray = 1;
+                    c.ray_kind = 1;
+                    return;
+                }
+            }
+        }
+        const double pn = sqrt(C[2]);
+        if (pn > 1e-300 && isfinite(pn)) {
+            const double inv = 1.0 / pn;
+            const double rate = C[4] * inv;
+            if (isfinite(rate) && rate < 0.0) {
+                const double viol = sqrt(C[3] + A3[2]) * inv;
+                if (viol / (-rate) <= o.infeasibility_tol) {
+                    finish(c, 2, kMsgUnbounded, true);
+                    c.save_ray = 2;
+                    c.ray_kind = 2;
+                    return;
+                }
+            }
+        }
+    }
+    if (is_optimal_best(c, o)) {
+        finish(c, 0, kMsgOptimal, true);
+        return;
+    }
+    double score;
+    const int choice = restart_choose(c, o, cur.kkt, avg.kkt, &score);
+    if (choice != 0) {
+        const bool from_avg = choice == 2 && have_avg;
+        update_weight(c.omega, o, sqrt(from_avg ? C[6] : C[5]), sqrt(from_avg ? R[8] : R[7]));
+        c.trial_omega = c.omega;
+        c.restart_src = from_avg ? 2 : 1;
+        if (from_avg) c.need_refresh = 1;
+        c.restart_baseline = score;
+        c.avg_weight = 0.0;
+        c.prev_candidate = INFINITY;
+        c.since_restart = 0;
+        ++c.restart_count;
+    }
+    loop_top_main(c, o, inf.n);
+}
+
+template <int V>
+__global__ void __launch_bounds__(kThreads) k_check_spmv(Global g, DeviceOptions o) {
+    const bool a_side = blockIdx.x < static_cast<unsigned>(g.a.num_ctas);
+    const int cta = a_side ? blockIdx.x : blockIdx.x - g.a.num_ctas;
+    const CtaWork cw = (a_side ? g.a.ctas : g.at.ctas)[cta];
+    InstanceCtl& c = g.ctl[cw.instance];
+    if (c.stage != kStageCheck || c.check_kind == kCheckTransition) return;
+    const InstanceInfo inf = g.info[cw.instance];
+    const bool have_avg = check_have_avg(c, o);
+    const bool rays =
+        (c.check_kind == kCheckMain || c.check_kind == kCheckEvaluate) && o.detect_infeasibility;
+
+    double acc[kCheckSlots];
+#pragma unroll
+    for (int q = 0; q < kCheckSlots; ++q) acc[q] = 0.0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (a_side) {   // rowPass (termination.cpp:66-135) for current/average, A*d for the primal ray
+        const double* xo = g.x_o + inf.col_off;
+        const double* xa = g.xa_o + inf.col_off;
+        const double* pp = g.p_proj + inf.col_off;
+        for (int s = cw.slice_begin + warp; s < cw.slice_end; s += kWarps) {
+            const SliceDesc sd = g.a.slices[s];
+            const LanePos lp = lane_pos(sd, lane);
+            const int len = lp.valid ? g.a.line_len[inf.a_len_base + lp.line] : 0;
+            double sum[3] = {0.0, 0.0, 0.0};
+            line_sums<V, 3>(inf.a_data_base + static_cast<int64_t>(sd.data_off) * 32, sd.steps,
+                            lp, lane, len, g.a.idx, g.a.val_orig, sum,
+                            [&](double (&a)[3], double v, int j) {
+                                a[0] += v * xo[j];
+                                if (have_avg) a[1] += v * xa[j];
+                                if (rays) a[2] += v * pp[j];
+                            });
+            if (lp.valid && lp.g == 0) {
+                const int64_t k = inf.row_off + lp.line;
+                const double lo = g.rl_orig[k], hi = g.ru_orig[k];
+                const double e0 = sum[0] - smax(lo, smin(sum[0], hi));
+                acc[0] += e0 * e0;
+                if (have_avg) {
+                    const double e1 = sum[1] - smax(lo, smin(sum[1], hi));
+                    acc[1] += e1 * e1;
+                }
+                if (rays) {
+                    double q = sum[2];
+                    if (isfinite(hi)) q = smin(q, 0.0);
+                    if (isfinite(lo)) q = smax(q, 0.0);
+                    const double drift = sum[2] - q;
+                    acc[2] += drift * drift;
+                }
+            }
+        }
+    } else {        // columnPass (termination.cpp:140-209), A'd for the dual ray
+        const double* yo = g.y_o + inf.row_off;
+        const double* ya = g.ya_o + inf.row_off;
+        const double* dy = g.dy_o + inf.row_off;
+        for (int s = cw.slice_begin + warp; s < cw.slice_end; s += kWarps) {
+            const SliceDesc sd = g.at.slices[s];
+            const LanePos lp = lane_pos(sd, lane);
+            const int len = lp.valid ? g.at.line_len[inf.at_len_base + lp.line] : 0;
+            double sum[3] = {0.0, 0.0, 0.0};
+            line_sums<V, 3>(inf.at_data_base + static_cast<int64_t>(sd.data_off) * 32, sd.steps,
+                            lp, lane, len, g.at.idx, g.at.val_orig, sum,
+                            [&](double (&a)[3], double v, int i) {
+                                a[0] += v * yo[i];
+                                if (have_avg) a[1] += v * ya[i];
+                                if (rays) a[2] += v * dy[i];
+                            });
+            if (lp.valid && lp.g == 0) {
+                const int64_t k = inf.col_off + lp.line;
+                const double co = g.c_orig[k];
+                const double lo = g.xl_orig[k], hi = g.xu_orig[k];
+                const bool lo_f = isfinite(lo), hi_f = isfinite(hi);
+                for (int which = 0; which < 2; ++which) {
+                    if (which == 1 && !have_avg) break;
+                    const double reduced = co + sum[which];
+                    double q = reduced;
+                    if (!lo_f) q = smin(q, 0.0);
+                    if (!hi_f) q = smax(q, 0.0);
+                    const double drift = reduced - q;
+                    acc[2 * which] += drift * drift;
+                    if (q > 0.0) acc[2 * which + 1] += q * lo;
+                    else if (q < 0.0) acc[2 * which + 1] += q * hi;
+                }
+                if (rays) {
+                    const double r = sum[2];
+                    double q = r;
+                    if (!lo_f) q = smin(q, 0.0);
+                    if (!hi_f) q = smax(q, 0.0);
+                    const double drift = r - q;
+                    acc[4] += drift * drift;
+                    if (q > 0.0) acc[5] += q * lo;
+                    else if (q < 0.0) acc[5] += q * hi;
+                }
+            }
+        }
+    }
+    block_sum<kCheckSlots>(acc);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < kCheckSlots; ++q)
+            g.part_check[static_cast<int64_t>(blockIdx.x) * kCheckSlots + q] = acc[q];
+    }
+    const int expected = (inf.a_cta_end - inf.a_cta_begin) + (inf.at_cta_end - inf.at_cta_begin);
+    if (!arrive_last(g.count_check + cw.instance, expected)) return;
+    if (threadIdx.x < 32) check_control(g, o, c, inf);
+}
+
+// ---------------------------------------------------------------------------
+// Check, application of the decisions
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_check_apply(Global g, Work<T> w) {
+    const VecWork vw = g.vec[blockIdx.x];
+    const InstanceCtl& c = g.ctl[vw.instance];
+    if (!(c.best_src || c.restart_src || c.to_polish || c.save_ray)) return;
+    if (!precision_matches<T>(c)) return;
+    const InstanceInfo inf = g.info[vw.instance];
+    const int p = c.parity;
+    if (!vw.is_row) {
+        for (int j = vw.begin + threadIdx.x; j < vw.end; j += blockDim.x) {
+            const int64_t k = inf.col_off + j;
+            if (c.best_src == 1) g.best_x[k] = g.x_o[k];
+            else if (c.best_src == 2) g.best_x[k] = g.xa_o[k];
+            if (c.save_ray == 2)
+                g.pray[k] = g.cs[k] * (static_cast<double>(w.X[p][k]) - static_cast<double>(w.rx[k]));
+            if (c.restart_src) {
+                if (c.restart_src == 2) w.X[p][k] = w.avg_x[k];
+                w.rx[k] = w.X[p][k];
+            }
+            if (c.to_polish) {   // toScaled (scaling.cpp:39-53)
+                w.X[p][k] = static_cast<T>(g.best_x[k] / g.cs[k]);
+            }
+        }
+    } else {
+        for (int i = vw.begin + threadIdx.x; i < vw.end; i += blockDim.x) {
+            const int64_t k = inf.row_off + i;
+            if (c.best_src == 1) g.best_y[k] = g.y_o[k];
+            else if (c.best_src == 2) g.best_y[k] = g.ya_o[k];
+            if (c.save_ray == 1) g.dray[k] = g.dy_o[k];
+            if (c.restart_src) {
+                if (c.restart_src == 2) w.Y[p][k] = w.avg_y[k];
+                w.ry[k] = w.Y[p][k];
+            }
+            if (c.to_polish) {
+                w.Y[p][k] = static_cast<T>(g.best_y[k] / g.rs[k]);
+            }
+        }
+    }
+}
+
+// A x for the current iterate of instances whose iterate was replaced
+// (CpuPdhgKernel::refreshActivity, pdhg_kernel.cpp:40-42).
+template <class T, int V>
+__global__ void __launch_bounds__(kThreads) k_refresh(Global g, Work<T> w) {
+    const CtaWork cw = g.a.ctas[blockIdx.x];
+    const InstanceCtl& c = g.ctl[cw.instance];
+    if (!c.need_refresh || !precision_matches<T>(c)) return;
+    const InstanceInfo inf = g.info[cw.instance];
+    const int p = c.parity;
+    const T* __restrict__ x = w.X[p] + inf.col_off;
+    T* __restrict__ ax = w.AX[p] + inf.row_off;
+    const T* vals = matrix_values<T>(g.a);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int s = cw.slice_begin + warp; s < cw.slice_end; s += kWarps) {
+        const SliceDesc sd = g.a.slices[s];
+        const LanePos lp = lane_pos(sd, lane);
+        const int len = lp.valid ? g.a.line_len[inf.a_len_base + lp.line] : 0;
+        T sum[1] = {T(0)};
+        line_sums<V, 1>(inf.a_data_base + static_cast<int64_t>(sd.data_off) * 32, sd.steps, lp,
+                        lane, len, g.a.idx, vals, sum,
+                        [&](T (&a)[1], T v, int j) { a[0] += v * x[j]; });
+        if (lp.valid && lp.g == 0) ax[lp.line] = sum[0];
+    }
+}
+
+__global__ void k_finalize(Global g, int32_t count, int32_t* active) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= count) return;
+    InstanceCtl& c = g.ctl[b];
+    if (c.phase != kPhaseDone && active != nullptr) atomicAdd(active, 1);
+    if (c.stage == kStageCheck && c.check_kind == kCheckTransition) c.stage = kStageTrial;
+    c.best_src = 0;
+    c.restart_src = 0;
+    c.need_refresh = 0;
+    c.to_polish = 0;
+    c.save_ray = 0;
+}
+
+// Mixed precision: the FP64 stage starts from the last FP32 restart point.
+__global__ void k_switch_fp64(Global g, Work<float> w32, Work<double> w64) {
+    const VecWork vw = g.vec[blockIdx.x];
+    const InstanceCtl& c = g.ctl[vw.instance];
+    if (!c.to_polish || !c.fp64_stage) return;   // reused flag: set with fp64_stage on the switch
+    const InstanceInfo inf = g.info[vw.instance];
+    const int p = c.parity;
+    if (!vw.is_row) {
+        for (int j = vw.begin + threadIdx.x; j < vw.end; j += blockDim.x) {
+            const int64_t k = inf.col_off + j;
+            const double v = static_cast<double>(w32.rx[k]);
+            w64.X[p][k] = v;
+            w64.rx[k] = v;
+        }
+    } else {
+        for (int i = vw.begin + threadIdx.x; i < vw.end; i += blockDim.x) {
+            const int64_t k = inf.row_off + i;
+            const double v = static_cast<double>(w32.ry[k]);
+            w64.Y[p][k] = v;
+            w64.ry[k] = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Setup: Ruiz equilibration (scaling.cpp:55-107). Row maxima over the A side
+// and column maxima over the A^T side read the same scale state, as the
+// reference's single sweep does; max is exact, so the scale vectors equal the
+// reference's bit for bit.
+// ---------------------------------------------------------------------------
+template <int V>
+__global__ void __launch_bounds__(kThreads) k_ruiz_max(Global g, int a_ctas) {
+    const bool a_side = blockIdx.x < static_cast<unsigned>(a_ctas);
+    const Side side = a_side ? g.a : g.at;
+    const CtaWork cw = side.ctas[a_side ? blockIdx.x : blockIdx.x - a_ctas];
+    const InstanceInfo inf = g.info[cw.instance];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const double* line_scale = a_side ? g.rs + inf.row_off : g.cs + inf.col_off;
+    const double* other = a_side ? g.cs + inf.col_off : g.rs + inf.row_off;
+    double* out = a_side ? g.row_tmp + inf.row_off : g.col_tmp + inf.col_off;
+    const int64_t dbase = a_side ? inf.a_data_base : inf.at_data_base;
+    const int64_t lbase = a_side ? inf.a_len_base : inf.at_len_base;
+    for (int s = cw.slice_begin + warp; s < cw.slice_end; s += kWarps) {
+        const SliceDesc sd = side.slices[s];
+        const LanePos lp = lane_pos(sd, lane);
+        const int len = lp.valid ? side.line_len[lbase + lp.line] : 0;
+        const double f = lp.valid ? line_scale[lp.line] : 0.0;
+        double mx = 0.0;
+        const int64_t base = dbase + static_cast<int64_t>(sd.data_off) * 32;
+        for (int st = 0; st < sd.steps; st += V) {
+            const int64_t pidx = base + static_cast<int64_t>(st) * 32 + lane * V;
+            int32_t id[V];
+            double v[V];
+            ld<V>(side.idx + pidx, id);
+            ld<V>(side.val_orig + pidx, v);
+#pragma unroll
+            for (int q = 0; q < V; ++q) {
+                const int k = ((st + q) << lp.glog) + lp.g;
+                if (k < len) {
+                    // |a_ij| * r_i * c_j, multiplied in the reference's order
+                    const double m = a_side ? fabs(v[q]) * f * other[id[q]]
+                                            : fabs(v[q]) * other[id[q]] * f;
+                    mx = smax(mx, m);
+                }
+            }
+        }
+        for (int o = (1 << lp.glog) >> 1; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(kFull, mx, o));
+        if (lp.valid && lp.g == 0) out[lp.line] = mx;
+    }
+}
+
+__global__ void k_ruiz_update(Global g) {
+    const VecWork vw = g.vec[blockIdx.x];
+    const InstanceInfo inf = g.info[vw.instance];
+    double* scale = vw.is_row ? g.rs + inf.row_off : g.cs + inf.col_off;
+    const double* mx = vw.is_row ? g.row_tmp + inf.row_off : g.col_tmp + inf.col_off;
+    for (int k = vw.begin + threadIdx.x; k < vw.end; k += blockDim.x) {
+        const double m = mx[k];
+        if (m > 1e-30) scale[k] /= sqrt(m);
+    }
+}
+
+// Scaled coefficients (SparseMatrix::scaled, sparse_matrix.cpp:243-274).
+template <int V>
+__global__ void __launch_bounds__(kThreads) k_scale_values(Global g, double* a_s64, double* at_s64,
+                                                        float* a_s32, float* at_s32, int a_ctas) {
+    const bool a_side = blockIdx.x < static_cast<unsigned>(a_ctas);
+    const Side side = a_side ? g.a : g.at;
+    const CtaWork cw = side.ctas[a_side ? blockIdx.x : blockIdx.x - a_ctas];
+    const InstanceInfo inf = g.info[cw.instance];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const double* line_scale = a_side ? g.rs + inf.row_off : g.cs + inf.col_off;
+    const double* other = a_side ? g.cs + inf.col_off : g.rs + inf.row_off;
+    double* out64 = a_side ? a_s64 : at_s64;
+    float* out32 = a_side ? a_s32 : at_s32;
+    const int64_t dbase = a_side ? inf.a_data_base : inf.at_data_base;
+    const int64_t lbase = a_side ? inf.a_len_base : inf.at_len_base;
+    for (int s = cw.slice_begin + warp; s < cw.slice_end; s += kWarps) {
+        const SliceDesc sd = side.slices[s];
+        const LanePos lp = lane_pos(sd, lane);
+        const int len = lp.valid ? side.line_len[lbase + lp.line] : 0;
+        const double f = lp.valid ? line_scale[lp.line] : 0.0;
+        const int64_t base = dbase + static_cast<int64_t>(sd.data_off) * 32;
+        for (int st = 0; st < sd.steps; ++st) {
+            const int64_t pidx = base + static_cast<int64_t>(st - st % V) * 32 + lane * V + st % V;
+            const int k = (st << lp.glog) + lp.g;
+            double r = 0.0;
+            if (k < len) r = side.val_orig[pidx] * (f * other[side.idx[pidx]]);
+            out64[pidx] = r;
+            if (out32) out32[pidx] = static_cast<float>(r);
+        }
+    }
+}
+
+// Pock-Chambolle (preconditioner.cpp:31-80): row and column L1 sums of the
+// scaled matrix, each over its own side.
+template <class T, int V>
+__global__ void __launch_bounds__(kThreads) k_precondition(Global g, Work<T> w, int a_ctas) {
+    const bool a_side = blockIdx.x < static_cast<unsigned>(a_ctas);
+    const Side side = a_side ? g.a : g.at;
+    const CtaWork cw = side.ctas[a_side ? blockIdx.x : blockIdx.x - a_ctas];
+    const InstanceInfo inf = g.info[cw.instance];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t dbase = a_side ? inf.a_data_base : inf.at_data_base;
+    const int64_t lbase = a_side ? inf.a_len_base : inf.at_len_base;
+    T* sc = a_side ? w.sigma + inf.row_off : w.tau + inf.col_off;
+    T* isc = a_side ? w.isigma + inf.row_off : w.itau + inf.col_off;
+    for (int s = cw.slice_begin + warp; s < cw.slice_end; s += kWarps) {
+        const SliceDesc sd = side.slices[s];
+        const LanePos lp = lane_pos(sd, lane);
+        const int len = lp.valid ? side.line_len[lbase + lp.line] : 0;
+        double sum[1] = {0.0};
+        line_sums<V, 1>(dbase + static_cast<int64_t>(sd.data_off) * 32, sd.steps, lp, lane, len,
+                        side.idx, side.val_s64, sum,
+                        [&](double (&a)[1], double v, int) { a[0] += fabs(v); });
+        if (lp.valid && lp.g == 0) {
+            const double scale = sum[0] > 1e-12 ? 1.0 / sum[0] : 1.0;
+            sc[lp.line] = static_cast<T>(scale);
+            isc[lp.line] = static_cast<T>(1.0 / scale);
+        }
+    }
+}
+
+__device__ __forceinline__ double scale_bound(double b, double f) { return isfinite(b) ? b * f : b; }
+
+__device__ __forceinline__ double initial_value(double lo, double hi) {   // pdlp_solver.cpp:30-41
+    if (lo <= 0.0 && 0.0 <= hi) return 0.0;
+    if (isfinite(lo)) return lo;
+    if (isfinite(hi)) return hi;
+    return 0.0;
+}
+
+// Scaled objective and bounds (scaling.cpp:109-135), the starting point
+// (pdlp_solver.cpp:168-176) or a warm start, and its cold alternative.
+template <class T>
+__global__ void k_setup_vectors(Global g, Work<T> w) {
+    const VecWork vw = g.vec[blockIdx.x];
+    const InstanceInfo inf = g.info[vw.instance];
+    const bool warm = g.warm_x != nullptr || g.warm_y != nullptr;
+    if (!vw.is_row) {
+        for (int j = vw.begin + threadIdx.x; j < vw.end; j += blockDim.x) {
+            const int64_t k = inf.col_off + j;
+            const double f = g.cs[k];
+            const double lo = scale_bound(g.xl_orig[k], 1.0 / f);
+            const double hi = scale_bound(g.xu_orig[k], 1.0 / f);
+            w.c[k] = static_cast<T>(g.c_orig[k] * f);
+            w.xl[k] = static_cast<T>(lo);
+            w.xu[k] = static_cast<T>(hi);
+            const double cold = initial_value(lo, hi);
+            double x0 = cold;
+            if (g.warm_x != nullptr) {
+                const double v = g.warm_x[k] / f;
+                x0 = isfinite(v) ? smax(lo, smin(v, hi)) : cold;
+            }
+            w.X[0][k] = static_cast<T>(x0);
+            w.X[1][k] = static_cast<T>(x0);
+            w.rx[k] = static_cast<T>(x0);
+            w.avg_x[k] = static_cast<T>(warm ? cold : 0.0);
+        }
+    } else {
+        for (int i = vw.begin + threadIdx.x; i < vw.end; i += blockDim.x) {
+            const int64_t k = inf.row_off + i;
+            const double f = g.rs[k];
+            w.rl[k] = static_cast<T>(scale_bound(g.rl_orig[k], f));
+            w.ru[k] = static_cast<T>(scale_bound(g.ru_orig[k], f));
+            double y0 = 0.0;
+            if (g.warm_y != nullptr) {
+                const double v = g.warm_y[k] / f;
+                y0 = isfinite(v) ? v : 0.0;
+            }
+            w.Y[0][k] = static_cast<T>(y0);
+            w.Y[1][k] = static_cast<T>(y0);
+            w.ry[k] = static_cast<T>(y0);
+            w.avg_y[k] = static_cast<T>(0.0);
+            w.AX[0][k] = T(0);
+            w.AX[1][k] = T(0);
+        }
+    }
+}
+
+// Shared-matrix batches: scales and preconditioner depend on A only, so the
+// vectors of instance 0 are copied to every other instance.
+__global__ void k_broadcast_scales(double* rs, double* cs, int64_t rows, int64_t cols, int32_t count) {
+    const int64_t total = (rows + cols) * (count - 1);
+    for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t b = 1 + t / (rows + cols), e = t % (rows + cols);
+        if (e < rows) rs[b * rows + e] = rs[e];
+        else cs[b * cols + (e - rows)] = cs[e - rows];
+    }
+}
+
+template <class T>
+__global__ void k_broadcast_precond(T* sigma, T* isigma, T* tau, T* itau, int64_t rows, int64_t cols,
+                                    int32_t count) {
+    const int64_t total = (rows + cols) * (count - 1);
+    for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t b = 1 + t / (rows + cols), e = t % (rows + cols);
+        if (e < rows) {
+            sigma[b * rows + e] = sigma[e];
+            isigma[b * rows + e] = isigma[e];
+        } else {
+            tau[b * cols + (e - rows)] = tau[e - rows];
+            itau[b * cols + (e - rows)] = itau[e - rows];
+        }
+    }
+}
+
+// Plain product over one side, lines in internal order.
+template <class T, int V>
+__global__ void __launch_bounds__(kThreads) k_spmv(Global g, int transpose, const T* vals,
+                                                   const T* v, T* out) {
+    const Side side = transpose ? g.at : g.a;
+    const CtaWork cw = side.ctas[blockIdx.x];
+    const InstanceInfo inf = g.info[cw.instance];
+    const T* src = v + (transpose ? inf.row_off : inf.col_off);
+    T* dst = out + (transpose ? inf.col_off : inf.row_off);
+    const int64_t dbase = transpose ? inf.at_data_base : inf.a_data_base;
+    const int64_t lbase = transpose ? inf.at_len_base : inf.a_len_base;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int s = cw.slice_begin + warp; s < cw.slice_end; s += kWarps) {
+        const SliceDesc sd = side.slices[s];
+        const LanePos lp = lane_pos(sd, lane);
+        const int len = lp.valid ? side.line_len[lbase + lp.line] : 0;
+        T sum[1] = {T(0)};
+        line_sums<V, 1>(dbase + static_cast<int64_t>(sd.data_off) * 32, sd.steps, lp, lane, len,
+                        side.idx, vals, sum, [&](T (&a)[1], T x, int j) { a[0] += x * src[j]; });
+        if (lp.valid && lp.g == 0) dst[lp.line] = sum[0];
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Power iteration on A'A (preconditioner.cpp:82-140), used only when the
+// diagonal preconditioner is off. Per-instance state lives in ctl.dbg:
+// [4] estimate, [5] previous, [6] scale 1/||z||, [7] state (0 running,
+// 1 converged, 2 stopped on a zero vector, 3 budget exhausted), [8] unit flag.
+// ---------------------------------------------------------------------------
+__global__ void k_power_dot(Global g, const double* x, const double* z) {
+    const VecWork vw = g.vec[blockIdx.x];
+    const InstanceInfo inf = g.info[vw.instance];
+    double acc[2] = {0.0, 0.0};
+    if (!vw.is_row && g.ctl[vw.instance].dbg[7] == 0.0) {
+        for (int j = vw.begin + threadIdx.x; j < vw.end; j += blockDim.x) {
+            const double a = x[inf.col_off + j], b = z[inf.col_off + j];
+            acc[0] += a * b;
+            acc[1] += b * b;
+        }
+    }
+    block_sum<2>(acc);
+    if (threadIdx.x == 0) {
+        g.part_prep[static_cast<int64_t>(blockIdx.x) * kPrepSlots] = acc[0];
+        g.part_prep[static_cast<int64_t>(blockIdx.x) * kPrepSlots + 1] = acc[1];
+    }
+}
+
+__global__ void k_power_step(Global g, int32_t count, int init, int it, int budget) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= count) return;
+    InstanceCtl& c = g.ctl[b];
+    if (c.dbg[7] != 0.0) return;
+    const InstanceInfo inf = g.info[b];
+    double xz = 0.0, zz = 0.0;
+    for (int k = inf.vec_cta_begin; k < inf.vec_cta_end; ++k) {
+        if (g.vec[k].is_row) continue;
+        xz += g.part_prep[static_cast<int64_t>(k) * kPrepSlots];
+        zz += g.part_prep[static_cast<int64_t>(k) * kPrepSlots + 1];
+    }
+    const double norm = sqrt(zz);
+    if (init) {
+        c.dbg[8] = norm == 0.0 ? 1.0 : 0.0;
+        c.dbg[6] = norm > 0.0 ? 1.0 / norm : 0.0;
+        return;
+    }
+    const double est = sqrt(smax(xz, 0.0));
+    c.dbg[4] = est;
+    if (norm == 0.0) {
+        c.dbg[7] = 2.0;
+        return;
+    }
+    c.dbg[6] = 1.0 / norm;
+    c.dbg[8] = 0.0;
+    if (it > 0 && est > 0.0 && fabs(est - c.dbg[5]) <= 1e-8 * est) {
+        c.dbg[7] = 1.0;
+        return;
+    }
+    c.dbg[5] = est;
+    if (it == budget - 1) c.dbg[7] = 3.0;
+}
+
+__global__ void k_power_scale(Global g, double* x, const double* z) {
+    const VecWork vw = g.vec[blockIdx.x];
+    if (vw.is_row) return;
+    const InstanceCtl& c = g.ctl[vw.instance];
+    if (c.dbg[7] != 0.0) return;
+    const InstanceInfo inf = g.info[vw.instance];
+    const double s = c.dbg[6];
+    const bool unit = c.dbg[8] != 0.0;
+    const double u = inf.n > 0 ? 1.0 / sqrt(static_cast<double>(inf.n)) : 0.0;
+    for (int j = vw.begin + threadIdx.x; j < vw.end; j += blockDim.x)
+        x[inf.col_off + j] = unit ? u : z[inf.col_off + j] * s;
+}
+
+// pdlp_solver.cpp:188-202 and the StepController constructor (step_controller.cpp:17-28).
+__global__ void k_power_finish(Global g, int32_t count, double safety, double min_scale) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= count) return;
+    InstanceCtl& c = g.ctl[b];
+    const double est = c.dbg[4];
+    const bool converged = c.dbg[7] == 1.0 || c.dbg[7] == 2.0;
+    const double safe = est > 0.0 ? 0.99 / (est * (converged ? 1.02 : 1.25)) : 1.0;
+    c.eta_max = safe;
+    c.eta = clampd(safety * safe, min_scale * safe, safe);
+    c.trial_eta = c.eta;
+    for (int q = 3; q < 12; ++q) c.dbg[q] = 0.0;
+}
+
+// The solve clock: the reference's clock starts when solve() is entered, so
+// the host's setup time is carried in.
+__global__ void k_stamp_clock(Global g, int32_t count, int64_t elapsed_ns, int64_t limit_ns) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= count) return;
+    InstanceCtl& c = g.ctl[b];
+    c.start_ns = now_ns() - elapsed_ns;
+    c.deadline_ns = limit_ns > 0 ? c.start_ns + limit_ns : 0;
+}
+
+inline unsigned blocks_for(int64_t n, int per) { return static_cast<unsigned>((n + per - 1) / per); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launch wrappers
+// ---------------------------------------------------------------------------
+template <class T>
+void launch_primal(const Global& g, const Work<T>& w, const DeviceOptions&, int vw, cudaStream_t s) {
+    if (g.at.num_ctas == 0) return;
+    switch (vw) {
+        case 4: k_primal<T, 4><<<g.at.num_ctas, kThreads, 0, s>>>(g, w); break;
+        case 2: k_primal<T, 2><<<g.at.num_ctas, kThreads, 0, s>>>(g, w); break;
+        default: k_primal<T, 1><<<g.at.num_ctas, kThreads, 0, s>>>(g, w); break;
+    }
+}
+
+template <class T>
+void launch_dual(const Global& g, const Work<T>& w, const DeviceOptions& o, int vw, cudaStream_t s) {
+    if (g.a.num_ctas == 0) return;
+    switch (vw) {
+        case 4: k_dual<T, 4><<<g.a.num_ctas, kThreads, 0, s>>>(g, w, o); break;
+        case 2: k_dual<T, 2><<<g.a.num_ctas, kThreads, 0, s>>>(g, w, o); break;
+        default: k_dual<T, 1><<<g.a.num_ctas, kThreads, 0, s>>>(g, w, o); break;
+    }
+}
+
+template <class T>
+void launch_check_prep(const Global& g, const Work<T>& w, const DeviceOptions& o, cudaStream_t s) {
+    if (g.num_vec) k_check_prep<T><<<g.num_vec, kThreads, 0, s>>>(g, w, o);
+}
+
+void launch_check_spmv(const Global& g, const DeviceOptions& o, int vw, cudaStream_t s) {
+    const int n = g.a.num_ctas + g.at.num_ctas;
+    if (n == 0) return;
+    switch (vw) {
+        case 4: k_check_spmv<4><<<n, kThreads, 0, s>>>(g, o); break;
+        case 2: k_check_spmv<2><<<n, kThreads, 0, s>>>(g, o); break;
+        default: k_check_spmv<1><<<n, kThreads, 0, s>>>(g, o); break;
+    }
+}
+
+template <class T>
+void launch_check_apply(const Global& g, const Work<T>& w, const DeviceOptions&, cudaStream_t s) {
+    if (g.num_vec) k_check_apply<T><<<g.num_vec, kThreads, 0, s>>>(g, w);
+}
+
+template <class T>
+void launch_refresh(const Global& g, const Work<T>& w, const DeviceOptions&, int vw, cudaStream_t s) {
+    if (g.a.num_ctas == 0) return;
+    switch (vw) {
+        case 4: k_refresh<T, 4><<<g.a.num_ctas, kThreads, 0, s>>>(g, w); break;
+        case 2: k_refresh<T, 2><<<g.a.num_ctas, kThreads, 0, s>>>(g, w); break;
+        default: k_refresh<T, 1><<<g.a.num_ctas, kThreads, 0, s>>>(g, w); break;
+    }
+}
+
+void launch_finalize(const Global& g, int32_t count, int32_t* active, cudaStream_t s) {
+    if (count) k_finalize<<<blocks_for(count, 256), 256, 0, s>>>(g, count, active);
+}
+
+void launch_switch_fp64(const Global& g, const Work<float>& w32, const Work<double>& w64,
+                        cudaStream_t s) {
+    if (g.num_vec) k_switch_fp64<<<g.num_vec, kThreads, 0, s>>>(g, w32, w64);
+}
+
+void launch_ruiz_max(const Global& g, int vw, int a_ctas, int at_ctas, cudaStream_t s) {
+    if (a_ctas + at_ctas == 0) return;
+    switch (vw) {
+        case 4: k_ruiz_max<4><<<a_ctas + at_ctas, kThreads, 0, s>>>(g, a_ctas); break;
+        case 2: k_ruiz_max<2><<<a_ctas + at_ctas, kThreads, 0, s>>>(g, a_ctas); break;
+        default: k_ruiz_max<1><<<a_ctas + at_ctas, kThreads, 0, s>>>(g, a_ctas); break;
+    }
+}
+
+void launch_ruiz_update(const Global& g, int vec_ctas, cudaStream_t s) {
+    if (vec_ctas) k_ruiz_update<<<vec_ctas, kThreads, 0, s>>>(g);
+}
+
+void launch_scale_values(const Global& g, double* a_s64, double* at_s64, float* a_s32,
+                         float* at_s32, int vw, int a_ctas, int at_ctas, cudaStream_t s) {
+    if (a_ctas + at_ctas == 0) return;
+    switch (vw) {
+        case 4: k_scale_values<4><<<a_ctas + at_ctas, kThreads, 0, s>>>(g, a_s64, at_s64, a_s32, at_s32, a_ctas); break;
+        case 2: k_scale_values<2><<<a_ctas + at_ctas, kThreads, 0, s>>>(g, a_s64, at_s64, a_s32, at_s32, a_ctas); break;
+        default: k_scale_values<1><<<a_ctas + at_ctas, kThreads, 0, s>>>(g, a_s64, at_s64, a_s32, at_s32, a_ctas); break;
+    }
+}
+
+template <class T>
+void launch_precondition(const Global& g, const Work<T>& w, int enabled, int vw, int a_ctas,
+                         int at_ctas, cudaStream_t s) {
+    if (!enabled || a_ctas + at_ctas == 0) return;
+    switch (vw) {
+        case 4: k_precondition<T, 4><<<a_ctas + at_ctas, kThreads, 0, s>>>(g, w, a_ctas); break;
+        case 2: k_precondition<T, 2><<<a_ctas + at_ctas, kThreads, 0, s>>>(g, w, a_ctas); break;
+        default: k_precondition<T, 1><<<a_ctas + at_ctas, kThreads, 0, s>>>(g, w, a_ctas); break;
+    }
+}
+
+template <class T>
+void launch_setup_vectors(const Global& g, const Work<T>& w, cudaStream_t s) {
+    if (g.num_vec) k_setup_vectors<T><<<g.num_vec, kThreads, 0, s>>>(g, w);
+}
+
+void launch_broadcast_scales(const Global& g, const InstanceInfo& first, int32_t count,
+                             int64_t rows, int64_t cols, cudaStream_t s) {
+    (void)first;
+    if (count > 1) k_broadcast_scales<<<592, 256, 0, s>>>(g.rs, g.cs, rows, cols, count);
+}
+
+template <class T>
+void launch_broadcast_precond(const Work<T>& w, const InstanceInfo&, int32_t count, int64_t rows,
+                              int64_t cols, cudaStream_t s) {
+    if (count > 1)
+        k_broadcast_precond<T><<<592, 256, 0, s>>>(w.sigma, w.isigma, w.tau, w.itau, rows, cols, count);
+}
+
+template <class T>
+void launch_spmv(const Global& g, int transpose, int values, const T* v, T* out, int vw,
+                 cudaStream_t s) {
+    const Side& side = transpose ? g.at : g.a;
+    if (side.num_ctas == 0) return;
+    const T* vals;
+    if constexpr (sizeof(T) == 8) {
+        vals = values == 0 ? side.val_orig : side.val_s64;
+    } else {
+        vals = side.val_s32;
+    }
+    switch (vw) {
+        case 4: k_spmv<T, 4><<<side.num_ctas, kThreads, 0, s>>>(g, transpose, vals, v, out); break;
+        case 2: k_spmv<T, 2><<<side.num_ctas, kThreads, 0, s>>>(g, transpose, vals, v, out); break;
+        default: k_spmv<T, 1><<<side.num_ctas, kThreads, 0, s>>>(g, transpose, vals, v, out); break;
+    }
+}
+
+void launch_power_dot(const Global& g, const double* x, const double* z, cudaStream_t s) {
+    if (g.num_vec) k_power_dot<<<g.num_vec, kThreads, 0, s>>>(g, x, z);
+}
+void launch_power_step(const Global& g, int32_t count, int init, int it, int budget, cudaStream_t s) {
+    if (count) k_power_step<<<blocks_for(count, 128), 128, 0, s>>>(g, count, init, it, budget);
+}
+void launch_power_scale(const Global& g, double* x, const double* z, cudaStream_t s) {
+    if (g.num_vec) k_power_scale<<<g.num_vec, kThreads, 0, s>>>(g, x, z);
+}
+void launch_power_finish(const Global& g, int32_t count, double safety, double min_scale, cudaStream_t s) {
+    if (count) k_power_finish<<<blocks_for(count, 128), 128, 0, s>>>(g, count, safety, min_scale);
+}
+void launch_stamp_clock(const Global& g, int32_t count, int64_t elapsed_ns, int64_t limit_ns, cudaStream_t s) {
+    if (count) k_stamp_clock<<<blocks_for(count, 128), 128, 0, s>>>(g, count, elapsed_ns, limit_ns);
+}
+
+#define PDLPGPU_INSTANTIATE(T)                                                                      \
+    template void launch_primal<T>(const Global&, const Work<T>&, const DeviceOptions&, int, cudaStream_t); \
+    template void launch_dual<T>(const Global&, const Work<T>&, const DeviceOptions&, int, cudaStream_t);   \
+    template void launch_check_prep<T>(const Global&, const Work<T>&, const DeviceOptions&, cudaStream_t);  \
+    template void launch_check_apply<T>(const Global&, const Work<T>&, const DeviceOptions&, cudaStream_t); \
+    template void launch_refresh<T>(const Global&, const Work<T>&, const DeviceOptions&, int, cudaStream_t); \
+    template void launch_precondition<T>(const Global&, const Work<T>&, int, int, int, int, cudaStream_t);  \
+    template void launch_setup_vectors<T>(const Global&, const Work<T>&, cudaStream_t);                    \
+    template void launch_broadcast_precond<T>(const Work<T>&, const InstanceInfo&, int32_t, int64_t, int64_t, cudaStream_t); \
+    template void launch_spmv<T>(const Global&, int, int, const T*, T*, int, cudaStream_t);
+
+PDLPGPU_INSTANTIATE(double)
+PDLPGPU_INSTANTIATE(float)
+
+}  // namespace pdlpgpu

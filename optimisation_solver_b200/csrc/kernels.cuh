@@ -1,0 +1,136 @@
+// kernels.cuh -- argument blocks and launch entry points of the device kernels.
+#pragma once
+
+#include "common.cuh"
+
+#include <cuda_runtime.h>
+
+namespace pdlpgpu {
+
+// One side of A in the SELL-G layout.
+struct Side {
+    const SliceDesc* slices;
+    const int32_t* idx;
+    const double* val_orig;      // original coefficients (FP64), used by the checks
+    const double* val_s64;       // Ruiz-scaled coefficients (FP64)
+    const float* val_s32;        // Ruiz-scaled coefficients (FP32), mixed precision only
+    const int32_t* line_len;
+    const CtaWork* ctas;
+    int32_t num_ctas;
+};
+
+// Arrays of one working precision (the scaled problem the iterations run on).
+template <class T>
+struct Work {
+    T* X[2];
+    T* Y[2];
+    T* AX[2];
+    T* avg_x;
+    T* avg_y;
+    T* rx;
+    T* ry;
+    T* c;
+    T* xl;
+    T* xu;
+    T* tau;
+    T* itau;
+    T* rl;
+    T* ru;
+    T* sigma;
+    T* isigma;
+};
+
+// Everything that does not depend on the working precision.
+struct Global {
+    InstanceCtl* ctl;
+    const InstanceInfo* info;
+    Side a, at;
+    const VecWork* vec;
+    int32_t num_vec;
+    int32_t shared_matrix;
+    // original problem (FP64) and the Ruiz scale vectors
+    double* rs;
+    double* cs;
+    const double* c_orig;
+    const double* xl_orig;
+    const double* xu_orig;
+    const double* rl_orig;
+    const double* ru_orig;
+    // check scratch and outputs (original coordinates)
+    double* x_o;
+    double* xa_o;
+    double* p_proj;
+    double* y_o;
+    double* ya_o;
+    double* dy_o;
+    double* best_x;
+    double* best_y;
+    double* dray;
+    double* pray;
+    // warm start (original coordinates), may be null
+    const double* warm_x;
+    const double* warm_y;
+    // setup scratch
+    double* row_tmp;
+    double* col_tmp;
+    // per-CTA partials and per-instance arrival counters
+    double* part_primal;
+    double* part_dual;
+    double* part_prep;
+    double* part_check;
+    int32_t* count_dual;
+    int32_t* count_check;
+};
+
+// --- launches (kernels.cu). `vw` is the vector width (1, 2 or 4). ---------
+
+template <class T>
+void launch_primal(const Global& g, const Work<T>& w, const DeviceOptions& o, int vw,
+                   cudaStream_t s);
+template <class T>
+void launch_dual(const Global& g, const Work<T>& w, const DeviceOptions& o, int vw,
+                 cudaStream_t s);
+template <class T>
+void launch_check_prep(const Global& g, const Work<T>& w, const DeviceOptions& o, cudaStream_t s);
+void launch_check_spmv(const Global& g, const DeviceOptions& o, int vw, cudaStream_t s);
+template <class T>
+void launch_check_apply(const Global& g, const Work<T>& w, const DeviceOptions& o, cudaStream_t s);
+template <class T>
+void launch_refresh(const Global& g, const Work<T>& w, const DeviceOptions& o, int vw,
+                    cudaStream_t s);
+void launch_finalize(const Global& g, int32_t count, int32_t* active, cudaStream_t s);
+void launch_switch_fp64(const Global& g, const Work<float>& w32, const Work<double>& w64,
+                        cudaStream_t s);
+
+// Setup. `a_ctas`/`at_ctas` limit the launch to the first CTAs of the maps
+// (instance 0 of a shared-matrix batch).
+void launch_ruiz_max(const Global& g, int vw, int a_ctas, int at_ctas, cudaStream_t s);
+void launch_ruiz_update(const Global& g, int vec_ctas, cudaStream_t s);
+void launch_scale_values(const Global& g, double* a_s64, double* at_s64, float* a_s32,
+                         float* at_s32, int vw, int a_ctas, int at_ctas, cudaStream_t s);
+template <class T>
+void launch_precondition(const Global& g, const Work<T>& w, int enabled, int vw, int a_ctas,
+                         int at_ctas, cudaStream_t s);
+template <class T>
+void launch_setup_vectors(const Global& g, const Work<T>& w, cudaStream_t s);
+void launch_broadcast_scales(const Global& g, const InstanceInfo& first, int32_t count,
+                             int64_t rows, int64_t cols, cudaStream_t s);
+template <class T>
+void launch_broadcast_precond(const Work<T>& w, const InstanceInfo& first, int32_t count,
+                              int64_t rows, int64_t cols, cudaStream_t s);
+
+void launch_power_dot(const Global& g, const double* x, const double* z, cudaStream_t s);
+void launch_power_step(const Global& g, int32_t count, int init, int it, int budget, cudaStream_t s);
+void launch_power_scale(const Global& g, double* x, const double* z, cudaStream_t s);
+void launch_power_finish(const Global& g, int32_t count, double safety, double min_scale,
+                         cudaStream_t s);
+void launch_stamp_clock(const Global& g, int32_t count, int64_t elapsed_ns, int64_t limit_ns,
+                        cudaStream_t s);
+
+// Plain products over the layout: out = A v (transpose = 0) or A^T v, lines
+// written in internal order. `values` selects orig (0), scaled FP64 (1), FP32 (2).
+template <class T>
+void launch_spmv(const Global& g, int transpose, int values, const T* v, T* out, int vw,
+                 cudaStream_t s);
+
+}  // namespace pdlpgpu

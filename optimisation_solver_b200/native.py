@@ -1,0 +1,164 @@
+"""ctypes binding of libpdlpgpu (include/pdlpgpu.h, include/pdlpgpu_components.h).
+
+The library is the product: there is no Python or CPU fallback. If it is not
+built, loading raises ``NativeLibraryMissing`` naming the build command.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libpdlpgpu.so")
+
+
+class NativeLibraryMissing(ImportError):
+    pass
+
+
+_dp = C.POINTER(C.c_double)
+_i64p = C.POINTER(C.c_int64)
+_i32p = C.POINTER(C.c_int32)
+
+
+class Lp(C.Structure):
+    _fields_ = [("num_rows", C.c_int32), ("num_cols", C.c_int32), ("row_start", _i64p),
+                ("col_index", _i32p), ("values", _dp), ("objective", _dp),
+                ("objective_offset", C.c_double), ("row_lower", _dp), ("row_upper", _dp),
+                ("var_lower", _dp), ("var_upper", _dp)]
+
+
+class Options(C.Structure):
+    _fields_ = [("iteration_limit", C.c_int64), ("time_limit_seconds", C.c_double),
+                ("primal_tolerance", C.c_double), ("dual_tolerance", C.c_double),
+                ("gap_tolerance", C.c_double), ("termination_check_frequency", C.c_int32),
+                ("power_iteration_count", C.c_int32), ("thread_count", C.c_int32),
+                ("parallel_nonzero_threshold", C.c_int64), ("initial_step_safety", C.c_double),
+                ("minimum_step_scale", C.c_double), ("maximum_primal_weight", C.c_double),
+                ("minimum_primal_weight", C.c_double), ("use_ruiz_scaling", C.c_int32),
+                ("ruiz_iterations", C.c_int32), ("detect_infeasibility", C.c_int32),
+                ("infeasibility_tolerance", C.c_double),
+                ("use_diagonal_preconditioning", C.c_int32),
+                ("use_adaptive_linesearch", C.c_int32), ("maximum_step_trials", C.c_int32),
+                ("use_averaging", C.c_int32), ("use_restarts", C.c_int32),
+                ("use_feasibility_polishing", C.c_int32),
+                ("minimum_restart_iterations", C.c_int32),
+                ("maximum_restart_iterations", C.c_int32),
+                ("restart_sufficient_decay", C.c_double), ("restart_necessary_decay", C.c_double),
+                ("restart_artificial_fraction", C.c_double),
+                ("initial_primal_weight", C.c_double), ("primal_weight_smoothing", C.c_double),
+                ("polishing_iterations", C.c_int32)]
+
+
+class ExtOptions(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("device", C.c_int32), ("lane_elements", C.c_int32),
+                ("vector_width", C.c_int32), ("chunk_slack", C.c_int32),
+                ("fp32_stall_checks", C.c_int32), ("fp32_switch_factor", C.c_int32),
+                ("disable_graphs", C.c_int32), ("reserved", C.c_int32 * 8)]
+
+
+class WarmStart(C.Structure):
+    _fields_ = [("primal", _dp), ("row_dual", _dp), ("primal_weight", C.c_double)]
+
+
+class Result(C.Structure):
+    _fields_ = [("status", C.c_int32), ("status_message", C.c_char * 160),
+                ("num_rows", C.c_int32), ("num_cols", C.c_int32), ("primal", _dp),
+                ("row_dual", _dp), ("dual_ray", _dp), ("primal_ray", _dp),
+                ("primal_objective", C.c_double), ("dual_objective", C.c_double),
+                ("primal_residual", C.c_double), ("dual_residual", C.c_double),
+                ("relative_gap", C.c_double), ("iterations", C.c_int64),
+                ("step_trials", C.c_int64), ("restart_count", C.c_int32),
+                ("solve_time_seconds", C.c_double), ("final_step_size", C.c_double),
+                ("static_step_bound", C.c_double), ("final_primal_weight", C.c_double),
+                ("precision_used", C.c_int32), ("fp64_iterations", C.c_int64),
+                ("device_seconds", C.c_double)]
+
+
+# Every symbol the public headers declare, with its signature.
+SIGNATURES = {
+    "pdlpgpu_default_options": (None, [C.POINTER(Options)]),
+    "pdlpgpu_default_ext_options": (None, [C.POINTER(ExtOptions)]),
+    "pdlpgpu_solve": (C.c_int32, [C.POINTER(Lp), C.POINTER(Options), C.POINTER(WarmStart),
+                                  C.POINTER(C.POINTER(Result))]),
+    "pdlpgpu_solve_ex": (C.c_int32, [C.POINTER(Lp), C.POINTER(Options), C.POINTER(ExtOptions),
+                                     C.POINTER(WarmStart), C.POINTER(C.POINTER(Result))]),
+    "pdlpgpu_solve_batch": (C.c_int32, [C.POINTER(C.POINTER(Lp)), C.c_int32, C.POINTER(Options),
+                                        C.POINTER(ExtOptions), C.POINTER(C.POINTER(WarmStart)),
+                                        C.POINTER(C.POINTER(Result))]),
+    "pdlpgpu_result_free": (None, [C.POINTER(Result)]),
+    "pdlpgpu_status_string": (C.c_char_p, [C.c_int32]),
+    "pdlpgpu_last_error": (C.c_char_p, []),
+    "pdlpgpu_device_count": (C.c_int32, []),
+    "pdlpgpu_spmv": (C.c_int32, [C.POINTER(Lp), C.c_int32, C.c_int32, _dp, _dp]),
+    "pdlpgpu_ruiz": (C.c_int32, [C.POINTER(Lp), C.c_int32, _dp, _dp, _dp]),
+    "pdlpgpu_precondition": (C.c_int32, [C.POINTER(Lp), _dp, _dp, _dp, _dp]),
+    "pdlpgpu_trial": (C.c_int32, [C.POINTER(Lp), C.c_int32] + [_dp] * 7 +
+                      [C.c_double, C.c_double] + [_dp] * 4),
+    "pdlpgpu_evaluate": (C.c_int32, [C.POINTER(Lp), C.c_double] + [_dp] * 6),
+    "pdlpgpu_layout_stats": (C.c_int32, [C.POINTER(Lp), C.POINTER(ExtOptions), _i64p]),
+    "pdlpgpu_layout_multiply": (C.c_int32, [C.POINTER(Lp), C.POINTER(ExtOptions), _dp, _dp]),
+}
+
+_LIB = None
+
+
+def lib():
+    """Loads libpdlpgpu.so once; raises NativeLibraryMissing if it is not built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise NativeLibraryMissing(
+                f"{LIB_PATH} is not built; run `python -m optimisation_solver_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def ptr(a, ctype=C.c_double):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ctype))
+
+
+class LpHandle:
+    """Holds the contiguous arrays of one LP alive while the C struct is used."""
+
+    def __init__(self, lp):
+        self.row_start = np.ascontiguousarray(lp.row_start, dtype=np.int64)
+        self.col_index = np.ascontiguousarray(lp.col_index, dtype=np.int32)
+        self.values = np.ascontiguousarray(lp.values, dtype=np.float64)
+        self.objective = np.ascontiguousarray(lp.objective, dtype=np.float64)
+        self.row_lower = np.ascontiguousarray(lp.row_lower, dtype=np.float64)
+        self.row_upper = np.ascontiguousarray(lp.row_upper, dtype=np.float64)
+        self.var_lower = np.ascontiguousarray(lp.var_lower, dtype=np.float64)
+        self.var_upper = np.ascontiguousarray(lp.var_upper, dtype=np.float64)
+        self.struct = Lp(int(lp.num_rows), int(lp.num_cols), ptr(self.row_start, C.c_int64),
+                         ptr(self.col_index, C.c_int32), ptr(self.values), ptr(self.objective),
+                         float(lp.objective_offset), ptr(self.row_lower), ptr(self.row_upper),
+                         ptr(self.var_lower), ptr(self.var_upper))
+
+
+def options_struct(options) -> Options:
+    o = Options()
+    lib().pdlpgpu_default_options(C.byref(o))
+    if options is not None:
+        for name, _ in Options._fields_:
+            setattr(o, name, type(getattr(o, name))(getattr(options, name)))
+    return o
+
+
+def ext_struct(**kw) -> ExtOptions:
+    e = ExtOptions()
+    lib().pdlpgpu_default_ext_options(C.byref(e))
+    for k, v in kw.items():
+        setattr(e, k, int(v))
+    return e
+
+
+def last_error() -> str:
+    return lib().pdlpgpu_last_error().decode()

@@ -1,0 +1,61 @@
+"""The C-ABI library loads on a host without a GPU and exports every symbol
+the public headers declare; host-only entry points work without a device."""
+import os
+import re
+
+import numpy as np
+
+from optimisation_solver_b200 import native
+from tests import cases
+
+INCLUDE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+
+
+def declared_symbols():
+    names = set()
+    for f in os.listdir(INCLUDE):
+        if f.endswith(".h"):
+            text = open(os.path.join(INCLUDE, f)).read()
+            names |= set(re.findall(r"\b(pdlpgpu_[a-z0-9_]+)\s*\(", text))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = native.lib()
+    names = declared_symbols()
+    assert names, "no declarations found"
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_every_declared_symbol():
+    assert declared_symbols() <= set(native.SIGNATURES)
+
+
+def test_status_strings_match_reference():
+    lib = native.lib()
+    names = ["optimal", "infeasible", "unbounded", "iteration_limit", "time_limit",
+             "numerical_failure", "invalid_problem"]
+    for code, name in enumerate(names):
+        assert lib.pdlpgpu_status_string(code).decode() == name
+    assert lib.pdlpgpu_status_string(99).decode() == "unknown"
+
+
+def test_default_options_match_reference(port_oracle):
+    o = native.options_struct(None)
+    ref = port_oracle.default_options()
+    for name, _ in native.Options._fields_:
+        assert getattr(o, name) == ref[name], name
+
+
+def test_device_count_without_gpu_is_safe():
+    assert native.lib().pdlpgpu_device_count() >= 0
+
+
+def test_invalid_problem_needs_no_device():
+    from optimisation_solver_b200.pdlp import PdlpSolver
+    from optimisation_solver_b200.lp import PdlpStatus
+    r = PdlpSolver().solve(cases.crossed_row_bounds(), cases.strict_options())
+    assert r.status == PdlpStatus.INVALID_PROBLEM
+    assert r.status_message == "Invalid row bounds"
+    assert r.primal.size == 0 and np.isnan(r.primal_objective)
