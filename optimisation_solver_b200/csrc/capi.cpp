@@ -5,6 +5,7 @@
 #include "engine.hpp"
 #include "pdlpgpu.h"
 #include "pdlpgpu_components.h"
+#include "pdlpgpu_session.h"
 
 #include <cmath>
 #include <cstdio>
@@ -373,6 +374,116 @@ int32_t pdlpgpu_layout_multiply(const pdlpgpu_lp* lp, const pdlpgpu_ext_options*
                     for (int g = 0; g < o; ++g) lane_sum[g] += lane_sum[g + o];
                 out[L.row_perm[line]] = lane_sum[0];
             }
+        }
+        return 0;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Sessions
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct pdlpgpu_session {
+    explicit pdlpgpu_session(int device) : engine(device) {}
+    pdlpgpu::Engine engine;
+};
+
+extern "C" {
+
+int32_t pdlpgpu_session_create(const pdlpgpu_lp* family, int32_t batch,
+                               const pdlpgpu_options* options,
+                               const pdlpgpu_ext_options* ext, pdlpgpu_session** session) {
+    if (family == nullptr || session == nullptr || batch <= 0) {
+        set_error("invalid session arguments");
+        return -1;
+    }
+    try {
+        const pdlpgpu_ext_options e = ext_or_default(ext);
+        auto* s = new pdlpgpu_session(e.device);
+        if (!s->engine.session_create(*family, batch, opt_or_default(options), e)) {
+            set_error(s->engine.error());
+            delete s;
+            *session = nullptr;
+            return -1;
+        }
+        *session = s;
+        return 0;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        *session = nullptr;
+        return -1;
+    }
+}
+
+void pdlpgpu_session_destroy(pdlpgpu_session* session) { delete session; }
+
+int32_t pdlpgpu_session_load(pdlpgpu_session* s, int32_t on_device, const double* objective,
+                             const double* row_lower, const double* row_upper,
+                             const double* var_lower, const double* var_upper,
+                             const double* warm_primal, const double* warm_dual,
+                             const double* warm_weight) {
+    if (s == nullptr) return -1;
+    try {
+        if (!s->engine.session_load(on_device != 0, objective, row_lower, row_upper, var_lower,
+                                    var_upper, warm_primal, warm_dual, warm_weight)) {
+            set_error(s->engine.error());
+            return -1;
+        }
+        return 0;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+int32_t pdlpgpu_session_solve(pdlpgpu_session* s) {
+    if (s == nullptr) return -1;
+    try {
+        int32_t optimal = 0;
+        if (!s->engine.session_solve(&optimal)) {
+            set_error(s->engine.error());
+            return -1;
+        }
+        return optimal;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+int32_t pdlpgpu_session_read(pdlpgpu_session* s, int32_t on_device, double* primal, double* dual,
+                             int32_t* status, int64_t* iterations, double* stats) {
+    if (s == nullptr) return -1;
+    try {
+        if (!s->engine.session_read(on_device != 0, primal, dual, status, iterations, stats)) {
+            set_error(s->engine.error());
+            return -1;
+        }
+        return 0;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+int32_t pdlpgpu_session_last_timing(pdlpgpu_session* s, double* device_seconds, int64_t* launches) {
+    if (s == nullptr) return -1;
+    if (device_seconds) *device_seconds = s->engine.device_seconds();
+    if (launches) *launches = s->engine.launches();
+    return 0;
+}
+
+int32_t pdlpgpu_session_time_kernels(pdlpgpu_session* s, int32_t reps, double* out) {
+    if (s == nullptr || reps <= 0) return -1;
+    try {
+        if (!s->engine.time_kernels(reps, out)) {
+            set_error(s->engine.error());
+            return -1;
         }
         return 0;
     } catch (const std::exception& ex) {

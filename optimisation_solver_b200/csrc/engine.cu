@@ -80,6 +80,7 @@ void fill_value(std::vector<T>& v, size_t n, T x) { v.assign(n, x); }
 Engine::Engine(int device) : device_(device) {}
 
 Engine::~Engine() {
+    for (void* q : extra_) cudaFree(q);
     if (graph_) cudaGraphExecDestroy(graph_);
     if (arena_) cudaFree(arena_);
     if (h_active_) cudaFreeHost(h_active_);
@@ -667,9 +668,11 @@ void Engine::enqueue_check_stage() {
 }
 
 void Engine::enqueue_chunk(int slots) {
+    // A mixed solve iterates in FP32; the FP64 trial kernels are captured only
+    // for the FP64 stage graph.
     for (int k = 0; k < slots; ++k) {
-        if (mixed_) enqueue_trial<float>(w32_);
-        enqueue_trial<double>(w64_);
+        if (mixed_ && !fp64_graph_) enqueue_trial<float>(w32_);
+        else enqueue_trial<double>(w64_);
     }
     enqueue_check_stage();
 }
@@ -697,8 +700,8 @@ bool Engine::run() {
     const int slack = spec_.ext.chunk_slack > 0 ? spec_.ext.chunk_slack : 4;
     const int slots = std::max(1, std::min(o.termination_check_frequency + slack, 1024));
     const bool graphs = spec_.ext.disable_graphs == 0;
-    if (*h_active_ != 0 && graphs && !build_graph(slots)) return false;
-    const int per_chunk = (mixed_ ? 4 : 2) * slots + (mixed_ ? 8 : 5);
+    if (*h_active_ != 0 && graphs && graph_ == nullptr && !build_graph(slots)) return false;
+    const int per_chunk = 2 * slots + (mixed_ ? 8 : 5);
     const int64_t trials_bound =
         (std::max<int64_t>(o.iteration_limit, 0) + std::max(o.polishing_iterations, 0) + 2) *
         std::max(o.maximum_step_trials, 1);
@@ -1028,6 +1031,211 @@ bool Engine::component_evaluate(const double* x, const double* y, const double* 
     metrics[6] = c.best_finite;
     metrics[7] = c.best_valid;
     for (int q = 0; q < 6; ++q) verdicts[q] = c.dbg[3 + q];
+    return true;
+}
+
+
+// ---------------------------------------------------------------------------
+// Sessions
+// ---------------------------------------------------------------------------
+bool Engine::session_create(const pdlpgpu_lp& family, int32_t batch, const pdlpgpu_options& opt,
+                            const pdlpgpu_ext_options& ext) {
+    family_ = family;
+    SolveSpec spec;
+    spec.lps.assign(static_cast<size_t>(batch), &family_);
+    spec.shared_matrix = true;
+    spec.opt = opt;
+    spec.ext = ext;
+    if (!prepare(spec)) return false;
+    if (count_ != batch) {
+        error_ = invalid_.empty() ? "invalid session" : invalid_[0];
+        return false;
+    }
+    const MatrixLayout& L = layouts_[0];
+    auto dalloc = [&](auto*& p, size_t count) {
+        void* q = nullptr;
+        if (!check(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(*p)), "cudaMalloc")) return false;
+        extra_.push_back(q);
+        p = static_cast<std::remove_reference_t<decltype(p)>>(q);
+        return true;
+    };
+    if (!dalloc(d_row_perm_, L.m) || !dalloc(d_col_perm_, L.n)) return false;
+    for (int k = 0; k < 5; ++k) if (!dalloc(fam_[k], (k == 0 || k >= 3) ? L.n : L.m)) return false;
+    if (!dalloc(warm_x_, static_cast<size_t>(cols_total_)) || !dalloc(warm_y_, static_cast<size_t>(rows_total_)) ||
+        !dalloc(warm_w_, static_cast<size_t>(batch)))
+        return false;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        return bytes == 0 || check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_), "upload");
+    };
+    std::vector<double> v;
+    bool ok = up(d_row_perm_, L.row_perm.data(), L.row_perm.size() * 4) &&
+              up(d_col_perm_, L.col_perm.data(), L.col_perm.size() * 4);
+    to_internal_cols(family.objective, v, 0);
+    ok = ok && up(fam_[0], v.data(), v.size() * 8);
+    to_internal_rows(family.row_lower, v, 0);
+    ok = ok && up(fam_[1], v.data(), v.size() * 8);
+    to_internal_rows(family.row_upper, v, 0);
+    ok = ok && up(fam_[2], v.data(), v.size() * 8);
+    to_internal_cols(family.var_lower, v, 0);
+    ok = ok && up(fam_[3], v.data(), v.size() * 8);
+    to_internal_cols(family.var_upper, v, 0);
+    ok = ok && up(fam_[4], v.data(), v.size() * 8);
+    if (!ok) return false;
+    // Matrix-only setup, once: Ruiz scaling, scaled coefficients,
+    // preconditioner, static step bound.
+    if (!init_control() || !setup_kernels()) return false;
+    if (!spec_.opt.use_diagonal_preconditioning) {
+        if (!power_iteration()) return false;
+        InstanceCtl c0;
+        if (!check(cudaMemcpyAsync(&c0, g_.ctl, sizeof(c0), cudaMemcpyDeviceToHost, stream_), "download") ||
+            !check(cudaStreamSynchronize(stream_), "power iteration"))
+            return false;
+        session_eta_max_ = c0.eta_max;
+    }
+    return check(cudaStreamSynchronize(stream_), "session setup");
+}
+
+bool Engine::session_load(bool on_device, const double* c, const double* rl, const double* ru,
+                          const double* xl, const double* xu, const double* wx, const double* wy,
+                          const double* ww) {
+    const int64_t n = info_[0].n, m = info_[0].m;
+    auto load = [&](const double* src, double* dst, const double* fam, bool cols) {
+        const int64_t len = cols ? n : m;
+        if (src == nullptr) {
+            launch_permute(fam, dst, nullptr, len, count_, 2, stream_);
+            return true;
+        }
+        const double* dsrc = src;
+        if (!on_device) {
+            double* staging = cols ? g_.x_o : g_.y_o;
+            if (!check(cudaMemcpyAsync(staging, src, static_cast<size_t>(len * count_) * 8,
+                                       cudaMemcpyHostToDevice, stream_), "load"))
+                return false;
+            dsrc = staging;
+        }
+        launch_permute(dsrc, dst, cols ? d_col_perm_ : d_row_perm_, len, count_, 0, stream_);
+        return true;
+    };
+    bool ok = load(c, const_cast<double*>(g_.c_orig), fam_[0], true) &&
+              load(rl, const_cast<double*>(g_.rl_orig), fam_[1], false) &&
+              load(ru, const_cast<double*>(g_.ru_orig), fam_[2], false) &&
+              load(xl, const_cast<double*>(g_.xl_orig), fam_[3], true) &&
+              load(xu, const_cast<double*>(g_.xu_orig), fam_[4], true);
+    g_.warm_x = nullptr;
+    g_.warm_y = nullptr;
+    if (wx != nullptr) ok = ok && load(wx, warm_x_, nullptr, true), g_.warm_x = warm_x_;
+    if (wy != nullptr) ok = ok && load(wy, warm_y_, nullptr, false), g_.warm_y = warm_y_;
+    session_warm_ = wx != nullptr || wy != nullptr;
+    session_has_ww_ = ww != nullptr;
+    if (ww != nullptr)
+        ok = ok && check(cudaMemcpyAsync(warm_w_, ww, static_cast<size_t>(count_) * 8,
+                                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                         stream_), "load");
+    return ok && check(cudaGetLastError(), "session load");
+}
+
+bool Engine::session_solve(int32_t* optimal) {
+    t0_ = std::chrono::steady_clock::now();
+    const pdlpgpu_options& o = spec_.opt;
+    launch_norm_parts(g_, stream_);
+    double initial_weight = o.initial_primal_weight;
+    launch_init_ctl(g_, dopt_, count_, mixed_ ? 1 : 0, session_warm_ ? 1 : 0,
+                    session_has_ww_ ? warm_w_ : nullptr, session_eta_max_, initial_weight,
+                    family_.objective_offset, stream_);
+    launch_setup_vectors<double>(g_, w64_, stream_);
+    if (mixed_) launch_setup_vectors<float>(g_, w32_, stream_);
+    launch_stamp_clock(g_, count_, 0,
+                       o.time_limit_seconds > 0.0 ? static_cast<int64_t>(o.time_limit_seconds * 1e9) : 0,
+                       stream_);
+    if (mixed_) launch_refresh<float>(g_, w32_, dopt_, tuning_.vector_width, stream_);
+    launch_refresh<double>(g_, w64_, dopt_, tuning_.vector_width, stream_);
+    const int64_t before = launches_;
+    enqueue_check_stage();
+    launches_ = before;
+    if (!check(cudaGetLastError(), "session start")) return false;
+    launches_ = 0;
+    if (!run()) return false;
+    std::vector<InstanceCtl> ctl(static_cast<size_t>(count_));
+    if (!check(cudaMemcpyAsync(ctl.data(), g_.ctl, ctl.size() * sizeof(InstanceCtl), cudaMemcpyDeviceToHost, stream_), "download") ||
+        !check(cudaStreamSynchronize(stream_), "session solve"))
+        return false;
+    int32_t k = 0;
+    for (const auto& c : ctl) k += (c.phase == kPhaseDone && c.status == 0) ? 1 : 0;
+    *optimal = k;
+    return true;
+}
+
+bool Engine::session_read(bool on_device, double* primal, double* dual, int32_t* status,
+                          int64_t* iterations, double* stats) {
+    const int64_t n = info_[0].n, m = info_[0].m;
+    if (primal != nullptr) {
+        double* dst = on_device ? primal : g_.x_o;
+        launch_permute(g_.best_x, dst, d_col_perm_, n, count_, 1, stream_);
+        if (!on_device && !check(cudaMemcpyAsync(primal, g_.x_o, static_cast<size_t>(n * count_) * 8,
+                                                 cudaMemcpyDeviceToHost, stream_), "read"))
+            return false;
+    }
+    if (dual != nullptr) {
+        double* dst = on_device ? dual : g_.y_o;
+        launch_permute(g_.best_y, dst, d_row_perm_, m, count_, 1, stream_);
+        if (!on_device && !check(cudaMemcpyAsync(dual, g_.y_o, static_cast<size_t>(m * count_) * 8,
+                                                 cudaMemcpyDeviceToHost, stream_), "read"))
+            return false;
+    }
+    if (status != nullptr || iterations != nullptr || stats != nullptr) {
+        std::vector<InstanceCtl> ctl(static_cast<size_t>(count_));
+        if (!check(cudaMemcpyAsync(ctl.data(), g_.ctl, ctl.size() * sizeof(InstanceCtl), cudaMemcpyDeviceToHost, stream_), "read") ||
+            !check(cudaStreamSynchronize(stream_), "read"))
+            return false;
+        for (int32_t b = 0; b < count_; ++b) {
+            const InstanceCtl& c = ctl[static_cast<size_t>(b)];
+            if (status) status[b] = c.phase == kPhaseDone ? c.status : PDLPGPU_NUMERICAL_FAILURE;
+            if (iterations) iterations[b] = c.iteration;
+            if (stats) {
+                double* st = stats + 6 * b;
+                st[0] = c.best_pobj; st[1] = c.best_dobj; st[2] = c.best_pres;
+                st[3] = c.best_dres; st[4] = c.best_gap; st[5] = static_cast<double>(c.step_trials);
+            }
+        }
+    }
+    return check(cudaStreamSynchronize(stream_), "read");
+}
+
+bool Engine::time_kernels(int reps, double* out) {
+    Global gm = g_;
+    gm.measure = 1;
+    cudaEvent_t e[4];
+    for (auto& ev : e) cudaEventCreate(&ev);
+    const int V = tuning_.vector_width;
+    auto primal = [&] { if (mixed_) launch_primal<float>(gm, w32_, dopt_, V, stream_); else launch_primal<double>(gm, w64_, dopt_, V, stream_); };
+    auto dual = [&] { if (mixed_) launch_dual<float>(gm, w32_, dopt_, V, stream_); else launch_dual<double>(gm, w64_, dopt_, V, stream_); };
+    primal();
+    dual();
+    cudaEventRecord(e[0], stream_);
+    for (int r = 0; r < reps; ++r) primal();
+    cudaEventRecord(e[1], stream_);
+    for (int r = 0; r < reps; ++r) dual();
+    cudaEventRecord(e[2], stream_);
+    if (!check(cudaEventSynchronize(e[2]), "time kernels")) return false;
+    float mp = 0.f, md = 0.f;
+    cudaEventElapsedTime(&mp, e[0], e[1]);
+    cudaEventElapsedTime(&md, e[1], e[2]);
+    for (auto& ev : e) cudaEventDestroy(ev);
+    // Algorithmic bytes: each nonzero once (value + index), every per-line
+    // vector once, the gathered vector once; a shared matrix counts once.
+    const double T = mixed_ ? 4.0 : 8.0;
+    double e_at = 0, e_a = 0, s_at = 0, s_a = 0;
+    for (const MatrixLayout& L : layouts_) {
+        e_at += L.at.entries; e_a += L.a.entries;
+        s_at += L.at.slots(); s_a += L.a.slots();
+    }
+    const double N = static_cast<double>(cols_total_), R = static_cast<double>(rows_total_);
+    out[0] = mp / reps;
+    out[1] = md / reps;
+    out[2] = e_at * (T + 4.0) + N * 7.0 * T + R * T;
+    out[3] = e_a * (T + 4.0) + R * 8.0 * T + N * T;
+    out[4] = s_at - e_at;
+    out[5] = s_a - e_a;
     return true;
 }
 

@@ -47,6 +47,18 @@ public:
     double device_seconds() const { return device_seconds_; }
     int64_t launches() const { return launches_; }
 
+    // --- sessions: one shared matrix, repeated batched solves --------------
+    bool session_create(const pdlpgpu_lp& family, int32_t batch, const pdlpgpu_options& opt,
+                        const pdlpgpu_ext_options& ext);
+    bool session_load(bool on_device, const double* c, const double* rl, const double* ru,
+                      const double* xl, const double* xu, const double* wx, const double* wy,
+                      const double* ww);
+    bool session_solve(int32_t* optimal);
+    bool session_read(bool on_device, double* primal, double* dual, int32_t* status,
+                      int64_t* iterations, double* stats);
+    bool time_kernels(int reps, double* out);
+    int32_t count() const { return count_; }
+
     // --- component tests (single instance, internal order handled here) ---
     bool component_spmv(int transpose, int values, const double* in, double* out);
     bool component_ruiz(double* row_scale, double* col_scale, double* scaled_csr);
@@ -112,7 +124,20 @@ private:
     double device_seconds_ = 0.0;
     int64_t launches_ = 0;
     bool ran_ = false;
+    bool fp64_graph_ = false;           // capturing the FP64-stage chunk of a mixed solve
     bool setup_ok_ = false;
+    // session state
+    std::vector<void*> extra_;              // device allocations beyond the arena
+    int32_t* d_row_perm_ = nullptr;
+    int32_t* d_col_perm_ = nullptr;
+    double* fam_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // c, rl, ru, xl, xu (internal)
+    double* warm_x_ = nullptr;
+    double* warm_y_ = nullptr;
+    double* warm_w_ = nullptr;
+    bool session_warm_ = false;
+    bool session_has_ww_ = false;
+    double session_eta_max_ = 0.99;
+    pdlpgpu_lp family_{};
 };
 
 const char* message_text(int32_t id);

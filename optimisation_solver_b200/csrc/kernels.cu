@@ -28,6 +28,7 @@
 #include "control.cuh"
 #include "kernels.cuh"
 
+#include <algorithm>
 #include <cstdio>
 
 namespace pdlpgpu {
@@ -192,11 +193,11 @@ template <class T, int V>
 __global__ void __launch_bounds__(kThreads) k_primal(Global g, Work<T> w) {
     const CtaWork cw = g.at.ctas[blockIdx.x];
     const InstanceCtl& c = g.ctl[cw.instance];
-    if (!trial_active<T>(c)) return;
+    if (!g.measure && !trial_active<T>(c)) return;
     const InstanceInfo inf = g.info[cw.instance];
     const int p = c.parity;
     const T mult = static_cast<T>(c.trial_eta / c.trial_omega);
-    const bool pending = c.pending_avg != 0;
+    const bool pending = !g.measure && c.pending_avg != 0;
     const T frac = static_cast<T>(c.avg_frac);
 
     const T* __restrict__ y = w.Y[p] + inf.row_off;
@@ -245,11 +246,11 @@ template <class T, int V>
 __global__ void __launch_bounds__(kThreads) k_dual(Global g, Work<T> w, DeviceOptions o) {
     const CtaWork cw = g.a.ctas[blockIdx.x];
     InstanceCtl& c = g.ctl[cw.instance];
-    if (!trial_active<T>(c)) return;
+    if (!g.measure && !trial_active<T>(c)) return;
     const InstanceInfo inf = g.info[cw.instance];
     const int p = c.parity;
     const T dm = static_cast<T>(c.trial_eta * c.trial_omega);
-    const bool pending = c.pending_avg != 0;
+    const bool pending = !g.measure && c.pending_avg != 0;
     const T frac = static_cast<T>(c.avg_frac);
 
     const T* __restrict__ xt = w.X[p ^ 1] + inf.col_off;
@@ -299,6 +300,7 @@ __global__ void __launch_bounds__(kThreads) k_dual(Global g, Work<T> w, DeviceOp
         g.part_dual[2 * blockIdx.x] = red[0];
         g.part_dual[2 * blockIdx.x + 1] = red[1];
     }
+    if (g.measure) return;
     if (!arrive_last(g.count_dual + cw.instance, inf.a_cta_end - inf.a_cta_begin)) return;
     if (threadIdx.x < 32) {
         const double pm = warp_range_sum(g.part_primal, inf.at_cta_begin, inf.at_cta_end, 1, 0);
@@ -1139,6 +1141,84 @@ __global__ void k_stamp_clock(Global g, int32_t count, int64_t elapsed_ns, int64
     c.deadline_ns = limit_ns > 0 ? c.start_ns + limit_ns : 0;
 }
 
+
+// ---------------------------------------------------------------------------
+// Sessions: order changes between the caller's layout and the internal one,
+// the TerminationChecker normalisers (termination.cpp:58-62) and the initial
+// control state, all on the device.
+// ---------------------------------------------------------------------------
+__global__ void k_permute(const double* __restrict__ src, double* __restrict__ dst,
+                          const int32_t* __restrict__ perm, int64_t len, int32_t count, int mode) {
+    const int64_t total = len * count;
+    for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t b = t / len, k = t - b * len;
+        if (mode == 0) dst[t] = src[b * len + perm[k]];
+        else if (mode == 1) dst[b * len + perm[k]] = src[t];
+        else dst[t] = src[k];
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_norm_parts(Global g) {
+    const VecWork vw = g.vec[blockIdx.x];
+    const InstanceInfo inf = g.info[vw.instance];
+    double acc[1] = {0.0};
+    if (!vw.is_row) {
+        for (int j = vw.begin + threadIdx.x; j < vw.end; j += blockDim.x) {
+            const double v = g.c_orig[inf.col_off + j];
+            acc[0] += v * v;
+        }
+    } else {
+        for (int i = vw.begin + threadIdx.x; i < vw.end; i += blockDim.x) {
+            const double l = g.rl_orig[inf.row_off + i], u = g.ru_orig[inf.row_off + i];
+            if (isfinite(l)) acc[0] += l * l;
+            if (isfinite(u) && u != l) acc[0] += u * u;
+        }
+    }
+    block_sum<1>(acc);
+    if (threadIdx.x == 0) g.part_prep[static_cast<int64_t>(blockIdx.x) * kPrepSlots] = acc[0];
+}
+
+// The host's init_control, per instance on the device.
+__global__ void k_init_ctl(Global g, DeviceOptions o, int32_t count, int32_t mixed, int32_t warm,
+                           const double* warm_weight, double eta_max, double initial_weight,
+                           double objective_offset) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= count) return;
+    const InstanceInfo inf = g.info[b];
+    double rows = 0.0, cols = 0.0;
+    for (int k = inf.vec_cta_begin; k < inf.vec_cta_end; ++k) {
+        const double v = g.part_prep[static_cast<int64_t>(k) * kPrepSlots];
+        if (g.vec[k].is_row) rows += v; else cols += v;
+    }
+    InstanceCtl c;
+    memset(&c, 0, sizeof(c));
+    c.phase = kPhaseMain;
+    c.stage = kStageCheck;
+    c.check_kind = kCheckInitial;
+    c.need_refresh = 1;
+    c.fp64_stage = mixed ? 0 : 1;
+    c.status = -1;
+    c.limit_status = 3;
+    c.have_avg_at_check = warm;
+    c.eta_max = eta_max;
+    c.eta = clampd(o.initial_step_safety * eta_max, o.min_step_scale * eta_max, eta_max);
+    c.omega = 1.0;
+    set_weight(c.omega, o, initial_weight);
+    if (warm_weight != nullptr && warm_weight[b] > 0.0) set_weight(c.omega, o, warm_weight[b]);
+    c.trial_eta = c.ctl_eta = c.eta;
+    c.trial_omega = c.ctl_omega = c.omega;
+    c.best_pobj = nan("");
+    c.best_dobj = -INFINITY;
+    c.best_pres = c.best_dres = c.best_gap = c.best_kkt = INFINITY;
+    c.restart_baseline = INFINITY;
+    c.prev_candidate = INFINITY;
+    c.pnorm = 1.0 + sqrt(rows);
+    c.dnorm = 1.0 + sqrt(cols);
+    c.objective_offset = objective_offset;
+    g.ctl[b] = c;
+}
+
 inline unsigned blocks_for(int64_t n, int per) { return static_cast<unsigned>((n + per - 1) / per); }
 
 }  // namespace
@@ -1289,6 +1369,24 @@ void launch_power_finish(const Global& g, int32_t count, double safety, double m
 }
 void launch_stamp_clock(const Global& g, int32_t count, int64_t elapsed_ns, int64_t limit_ns, cudaStream_t s) {
     if (count) k_stamp_clock<<<blocks_for(count, 128), 128, 0, s>>>(g, count, elapsed_ns, limit_ns);
+}
+
+void launch_permute(const double* src, double* dst, const int32_t* perm, int64_t len,
+                    int32_t count, int mode, cudaStream_t s) {
+    const int64_t total = len * count;
+    if (total == 0) return;
+    const unsigned blocks = static_cast<unsigned>(std::min<int64_t>((total + 255) / 256, 148 * 16));
+    k_permute<<<blocks, 256, 0, s>>>(src, dst, perm, len, count, mode);
+}
+void launch_norm_parts(const Global& g, cudaStream_t s) {
+    if (g.num_vec) k_norm_parts<<<g.num_vec, kThreads, 0, s>>>(g);
+}
+void launch_init_ctl(const Global& g, const DeviceOptions& o, int32_t count, int32_t mixed,
+                     int32_t warm, const double* warm_weight, double eta_max,
+                     double initial_weight, double objective_offset, cudaStream_t s) {
+    if (count)
+        k_init_ctl<<<blocks_for(count, 128), 128, 0, s>>>(g, o, count, mixed, warm, warm_weight,
+                                                          eta_max, initial_weight, objective_offset);
 }
 
 #define PDLPGPU_INSTANTIATE(T)                                                                      \

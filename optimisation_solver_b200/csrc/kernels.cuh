@@ -80,6 +80,9 @@ struct Global {
     double* part_check;
     int32_t* count_dual;
     int32_t* count_check;
+    // 1: timing mode -- every instance runs its trial kernels, no decision is
+    // taken and no state changes (the trial buffers are scratch).
+    int32_t measure;
 };
 
 // --- launches (kernels.cu). `vw` is the vector width (1, 2 or 4). ---------
@@ -126,6 +129,17 @@ void launch_power_finish(const Global& g, int32_t count, double safety, double m
                          cudaStream_t s);
 void launch_stamp_clock(const Global& g, int32_t count, int64_t elapsed_ns, int64_t limit_ns,
                         cudaStream_t s);
+
+// Sessions (one shared matrix; instance b's vectors at b*m / b*n).
+// mode 0: dst[b][k] = src[b][perm[k]]   (original -> internal)
+// mode 1: dst[b][perm[k]] = src[b][k]   (internal -> original)
+// mode 2: dst[b][k] = src[k]           (broadcast one internal vector)
+void launch_permute(const double* src, double* dst, const int32_t* perm, int64_t len,
+                    int32_t count, int mode, cudaStream_t s);
+void launch_norm_parts(const Global& g, cudaStream_t s);
+void launch_init_ctl(const Global& g, const DeviceOptions& o, int32_t count, int32_t mixed,
+                     int32_t warm, const double* warm_weight, double eta_max,
+                     double initial_weight, double objective_offset, cudaStream_t s);
 
 // Plain products over the layout: out = A v (transpose = 0) or A^T v, lines
 // written in internal order. `values` selects orig (0), scaled FP64 (1), FP32 (2).

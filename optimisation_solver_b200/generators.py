@@ -16,10 +16,12 @@ stress_lp           large_lp's matrix at m=100k, n=200k, with 20% free
                     log-uniform factors in [1e-4, 1e4] after planting.
 uneven_batch        1024 planted_lp instances, seed i for instance i, m
                     log-uniform in [200, 50000], n = 2m, degree U{4..12}.
-network_flow_family min-cost flow on a fixed geometric graph (2000 nodes, arcs to
-                    the 5 nearest neighbours in both directions, capacities
-                    U(5,50)); per instance a random feasible flow fixes the
-                    supplies and costs are length x lognormal(0, 0.2).
+network_flow_family min-cost flow on a fixed geometric graph (2000 nodes; for
+                    every node and each of its 5 nearest neighbours one arc in
+                    each direction, so 20,000 arcs with parallel arcs kept as
+                    separate columns; capacities U(5,50)); per instance a random
+                    feasible flow fixes the supplies and costs are length x
+                    lognormal(0, 0.2).
 
 Planting: with shadow prices y (c = A'y + z), a <= row that is tight has
 y <= 0, a slack row has y = 0, an equality row has any y; z >= 0 where x sits
@@ -235,8 +237,8 @@ def flow_graph(nodes=2000, neighbours=5, seed=0) -> FlowGraph:
     dst = nn.ravel()
     tail = np.concatenate([src, dst])
     head = np.concatenate([dst, src])
-    key = np.unique(tail * nodes + head)
-    tail, head = key // nodes, key % nodes
+    order = np.argsort(tail * nodes + head, kind="stable")   # arcs grouped by (tail, head)
+    tail, head = tail[order], head[order]
     length = np.sqrt(((pts[tail] - pts[head]) ** 2).sum(-1))
     capacity = rng.uniform(5.0, 50.0, tail.size)
     arcs = tail.size

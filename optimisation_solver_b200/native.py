@@ -100,6 +100,15 @@ SIGNATURES = {
     "pdlpgpu_evaluate": (C.c_int32, [C.POINTER(Lp), C.c_double] + [_dp] * 6),
     "pdlpgpu_layout_stats": (C.c_int32, [C.POINTER(Lp), C.POINTER(ExtOptions), _i64p]),
     "pdlpgpu_layout_multiply": (C.c_int32, [C.POINTER(Lp), C.POINTER(ExtOptions), _dp, _dp]),
+    "pdlpgpu_session_create": (C.c_int32, [C.POINTER(Lp), C.c_int32, C.POINTER(Options),
+                                           C.POINTER(ExtOptions), C.POINTER(C.c_void_p)]),
+    "pdlpgpu_session_destroy": (None, [C.c_void_p]),
+    "pdlpgpu_session_load": (C.c_int32, [C.c_void_p, C.c_int32] + [C.c_void_p] * 8),
+    "pdlpgpu_session_solve": (C.c_int32, [C.c_void_p]),
+    "pdlpgpu_session_read": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                         _i32p, _i64p, _dp]),
+    "pdlpgpu_session_last_timing": (C.c_int32, [C.c_void_p, _dp, _i64p]),
+    "pdlpgpu_session_time_kernels": (C.c_int32, [C.c_void_p, C.c_int32, _dp]),
 }
 
 _LIB = None

@@ -1,0 +1,109 @@
+"""Repeated batched solves of one LP family (include/pdlpgpu_session.h).
+
+A ``Session`` fixes the constraint matrix and the batch size; each ``solve``
+loads per-instance vectors -- numpy arrays (host) or device pointers such as
+``torch.Tensor.data_ptr()`` of CUDA tensors already in HBM -- and solves every
+instance to completion on the device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import native
+from .lp import CompiledLp, PdlpOptions, PdlpStatus
+
+_PRECISIONS = {"fp64": 0, "mixed": 1}
+
+
+def _addr(a):
+    """Address of a host numpy array, an integer device pointer, a CUDA tensor, or None."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return C.c_void_p(a)
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return C.c_void_p(a.ctypes.data)
+
+
+class Session:
+    def __init__(self, family: CompiledLp, batch: int, options: PdlpOptions | None = None,
+                 precision: str = "fp64", device: int = 0, **tuning):
+        self.family = family
+        self.batch = int(batch)
+        self.n, self.m = family.num_cols, family.num_rows
+        self._h = native.LpHandle(family)
+        self._o = native.options_struct(options or PdlpOptions())
+        self._e = native.ext_struct(precision=_PRECISIONS[precision], device=device, **tuning)
+        self._s = C.c_void_p()
+        rc = native.lib().pdlpgpu_session_create(C.byref(self._h.struct), self.batch,
+                                                 C.byref(self._o), C.byref(self._e),
+                                                 C.byref(self._s))
+        if rc != 0:
+            raise RuntimeError(f"session_create failed: {native.last_error()}")
+        self._keep = []
+
+    def close(self):
+        if self._s:
+            native.lib().pdlpgpu_session_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load(self, objective=None, row_lower=None, row_upper=None, var_lower=None,
+             var_upper=None, warm_primal=None, warm_dual=None, warm_weight=None,
+             on_device: bool = False):
+        arrs = [objective, row_lower, row_upper, var_lower, var_upper, warm_primal, warm_dual,
+                warm_weight]
+        if not on_device:
+            arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
+        self._keep = arrs
+        rc = native.lib().pdlpgpu_session_load(self._s, int(on_device), *[_addr(a) for a in arrs])
+        if rc != 0:
+            raise RuntimeError(f"session_load failed: {native.last_error()}")
+
+    def solve(self) -> int:
+        k = native.lib().pdlpgpu_session_solve(self._s)
+        if k < 0:
+            raise RuntimeError(f"session_solve failed: {native.last_error()}")
+        return k
+
+    def read(self, primal=None, dual=None, on_device: bool = False):
+        """Statuses, iterations and stats on the host; primal/dual into the
+        given buffers (allocated on the host when None and on_device is False)."""
+        if not on_device:
+            if primal is None:
+                primal = np.zeros((self.batch, self.n))
+            if dual is None:
+                dual = np.zeros((self.batch, self.m))
+        status = np.zeros(self.batch, dtype=np.int32)
+        iters = np.zeros(self.batch, dtype=np.int64)
+        stats = np.zeros((self.batch, 6))
+        rc = native.lib().pdlpgpu_session_read(self._s, int(on_device), _addr(primal), _addr(dual),
+                                               native.ptr(status, C.c_int32),
+                                               native.ptr(iters, C.c_int64), native.ptr(stats))
+        if rc != 0:
+            raise RuntimeError(f"session_read failed: {native.last_error()}")
+        return dict(primal=primal, dual=dual, status=[PdlpStatus(int(s)) for s in status],
+                    iterations=iters, primal_objective=stats[:, 0], dual_objective=stats[:, 1],
+                    primal_residual=stats[:, 2], dual_residual=stats[:, 3],
+                    relative_gap=stats[:, 4], step_trials=stats[:, 5].astype(np.int64))
+
+    def last_timing(self):
+        s, n = C.c_double(), C.c_int64()
+        native.lib().pdlpgpu_session_last_timing(self._s, C.byref(s), C.byref(n))
+        return s.value, n.value
+
+    def time_kernels(self, reps: int = 20) -> dict:
+        out = np.zeros(6)
+        rc = native.lib().pdlpgpu_session_time_kernels(self._s, reps, native.ptr(out))
+        if rc != 0:
+            raise RuntimeError(f"time_kernels failed: {native.last_error()}")
+        return dict(primal_ms=out[0], dual_ms=out[1], primal_bytes=out[2], dual_bytes=out[3],
+                    at_padding=out[4], a_padding=out[5])
