@@ -43,6 +43,33 @@ int32_t pdlpgpu_trial(const pdlpgpu_lp* lp, int32_t precision, const double* tau
                       const double* ax, double step, double weight, double* x_out,
                       double* y_out, double* ax_out, double* reductions);
 
+/* No counterpart in the reference. The fused trial of pdlpgpu_trial for
+ * callers that cannot let the library allocate device memory: a process that
+ * owns all device memory through its own pool and budget, or a loop that must
+ * not take the device-wide synchronisation of cudaMalloc. Every pointer is
+ * device memory the caller owns: A and A^T as CSR (int64 starts, int32
+ * indices, FP64 values), the vectors of pdlpgpu_trial, the outputs, and
+ * `reductions` (3 doubles: sum dx^2/tau, sum dy^2/sigma, dy'A dx). `stream`
+ * is a cudaStream_t (NULL = default stream); the call only enqueues work.
+ * Scratch is a fixed 192 KiB static device array inside the library, so rows
+ * and columns are limited to 8,388,608 each (larger sizes are rejected with an
+ * error). The first call on a device looks up that array's address, so make
+ * the first call on each device before any stream capture. All calls share
+ * the array: calls that overlap on the GPU race; each call writes every slot
+ * it later reads, so nothing needs clearing between calls. Returns 0, or -1
+ * with pdlpgpu_last_error() set. */
+int32_t pdlpgpu_trial_noalloc(int32_t rows, int32_t cols, const int64_t* a_row_start,
+                              const int32_t* a_col_index, const double* a_values,
+                              const int64_t* at_row_start, const int32_t* at_col_index,
+                              const double* at_values, const double* objective,
+                              const double* var_lower, const double* var_upper,
+                              const double* tau, const double* tau_inverse,
+                              const double* row_lower, const double* row_upper,
+                              const double* sigma, const double* sigma_inverse,
+                              const double* x, const double* y, const double* ax, double step,
+                              double weight, double* x_out, double* y_out, double* ax_out,
+                              double* reductions, void* stream);
+
 /* TerminationChecker::evaluate (pdlp_engine/src/termination.cpp:211-325) of
  * (x, y), and InfeasibilityDetector::testDualRay / testPrimalRay
  * (pdlp_engine/src/infeasibility.cpp:51-192) of the directions y - ry and

@@ -178,6 +178,9 @@ const char* pdlpgpu_status_string(int32_t status) {
 
 const char* pdlpgpu_last_error(void) { return g_last_error.c_str(); }
 
+// Lets the other translation units report through pdlpgpu_last_error.
+void pdlpgpu_internal_set_error(const char* message) { set_error(message ? message : ""); }
+
 int32_t pdlpgpu_device_count(void) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess) {

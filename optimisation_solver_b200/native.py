@@ -98,6 +98,8 @@ SIGNATURES = {
     "pdlpgpu_trial": (C.c_int32, [C.POINTER(Lp), C.c_int32] + [_dp] * 7 +
                       [C.c_double, C.c_double] + [_dp] * 4),
     "pdlpgpu_evaluate": (C.c_int32, [C.POINTER(Lp), C.c_double] + [_dp] * 6),
+    "pdlpgpu_trial_noalloc": (C.c_int32, [C.c_int32, C.c_int32] + [C.c_void_p] * 18 +
+                              [C.c_double, C.c_double] + [C.c_void_p] * 5),
     "pdlpgpu_layout_stats": (C.c_int32, [C.POINTER(Lp), C.POINTER(ExtOptions), _i64p]),
     "pdlpgpu_layout_multiply": (C.c_int32, [C.POINTER(Lp), C.POINTER(ExtOptions), _dp, _dp]),
     "pdlpgpu_session_create": (C.c_int32, [C.POINTER(Lp), C.c_int32, C.POINTER(Options),
