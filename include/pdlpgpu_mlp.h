@@ -1,0 +1,73 @@
+/*
+ * pdlpgpu_mlp.h -- the learned warm start: a 3-layer MLP (BF16 weights and
+ * activations, FP32 accumulation) that maps an LP instance's parameters to a
+ * starting point (x0, y0) and an initial primal weight, trained on the device
+ * by this library's own tcgen05 tensor-core GEMM, backward and Adam kernels.
+ *
+ * No counterpart in the reference: its PdlpSolver::solve always starts from
+ * the box projection of 0 and y = 0 with the option's primal weight
+ * (pdlp_engine/src/pdlp_solver.cpp:168-176, pdlp_options.h:61-71). The solver
+ * then runs from the prediction to the same tolerance; the better of the
+ * prediction and the cold start by KKT score is used (pdlpgpu_warmstart).
+ *
+ * All tensors are device pointers, row-major:
+ *   inputs   [batch][in]   BF16 (uint16 bit patterns)
+ *   outputs  [batch][out]  FP32
+ *   targets  [batch][out]  FP32, with per-output loss weights [out]
+ * `in` must be a multiple of 8; `out` and `hidden` multiples of 64.
+ */
+#ifndef PDLPGPU_MLP_H
+#define PDLPGPU_MLP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pdlpgpu_mlp pdlpgpu_mlp;
+
+/* Weights He-initialised from `seed`; Adam state zero. Returns 0 or -1. */
+int32_t pdlpgpu_mlp_create(int32_t in, int32_t hidden, int32_t out, int32_t batch,
+                           uint64_t seed, int32_t device, pdlpgpu_mlp** mlp);
+void pdlpgpu_mlp_destroy(pdlpgpu_mlp* mlp);
+
+/* outputs = W3 relu(W2 relu(W1 x + b1) + b2) + b3 for `batch` rows. */
+int32_t pdlpgpu_mlp_forward(pdlpgpu_mlp* mlp, const uint16_t* inputs, float* outputs);
+
+/* One Adam step on the weighted mean-squared error
+ * loss = (1/batch) sum_b sum_j w_j (out_bj - target_bj)^2.
+ * Writes the loss (before the step) to *loss when non-NULL. */
+int32_t pdlpgpu_mlp_train_step(pdlpgpu_mlp* mlp, const uint16_t* inputs, const float* targets,
+                               const float* loss_weights, float learning_rate, float* loss);
+
+/* Gradients of the loss at the current weights without updating them (for
+ * gradient checks): device FP32 buffers shaped like the parameters, any may
+ * be NULL. */
+int32_t pdlpgpu_mlp_gradients(pdlpgpu_mlp* mlp, const uint16_t* inputs, const float* targets,
+                              const float* loss_weights, float* dW1, float* db1, float* dW2,
+                              float* db2, float* dW3, float* db3, float* loss);
+
+/* Copies the FP32 master parameters out of / into the model (device
+ * pointers, shapes W1 [hidden][in], b1 [hidden], W2 [hidden][hidden],
+ * b2 [hidden], W3 [out][hidden], b3 [out]; NULL skips a tensor). Setting
+ * refreshes the BF16 copies the GEMMs read. */
+int32_t pdlpgpu_mlp_get_params(pdlpgpu_mlp* mlp, float* W1, float* b1, float* W2, float* b2,
+                               float* W3, float* b3);
+int32_t pdlpgpu_mlp_set_params(pdlpgpu_mlp* mlp, const float* W1, const float* b1,
+                               const float* W2, const float* b2, const float* W3, const float* b3);
+
+/* The tensor-core GEMM alone: C[M][N] (FP32) = A[M][K] * B[N][K]^T with A, B
+ * BF16 row-major (K contiguous), K a multiple of 8, split over `splits`
+ * K-ranges summed in a fixed order. Device pointers; returns 0 or -1. */
+int32_t pdlpgpu_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint16_t* A, const uint16_t* B,
+                          float* C, int32_t splits);
+
+/* Kernel launches issued by the last forward / train step of `mlp`. */
+int64_t pdlpgpu_mlp_launches(pdlpgpu_mlp* mlp);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -182,7 +182,7 @@ __device__ inline void average_add(InstanceCtl& c, double weight) {   // iterate
 
 // After the two halves of one trial: finiteness test, linesearch decision,
 // commit, averaging and the check boundary.
-__device__ inline void trial_control(InstanceCtl& c, const DeviceOptions& o, double pmove,
+__device__ __noinline__ void trial_control(InstanceCtl& c, const DeviceOptions& o, double pmove,
                                      double dmove, double inter, int32_t n_cols) {
     c.pending_avg = 0;
     c.dbg[0] = pmove;

@@ -87,22 +87,39 @@ __device__ __forceinline__ LanePos lane_pos(const SliceDesc& sd, int lane) {
 
 // Sum of NQ products over the lane's entries of one line, then combined over
 // the G lanes of the line with an xor butterfly (every lane ends with the same
-// bits, so the result is deterministic).
+// bits, so the result is deterministic). Up to kDepth vector loads of index
+// and value are issued before their gathers, so a lane keeps several
+// independent memory requests in flight instead of one load-gather chain.
 template <int V, int NQ, class TA, class TV, class F>
 __device__ __forceinline__ void line_sums(int64_t base, int steps, const LanePos& lp, int lane,
                                           int len, const int32_t* __restrict__ idx,
                                           const TV* __restrict__ val, TA (&acc)[NQ], F fetch) {
-#pragma unroll 2
-    for (int s = 0; s < steps; s += V) {
-        const int64_t p = base + static_cast<int64_t>(s) * 32 + lane * V;
-        int32_t id[V];
-        TV v[V];
-        ld<V>(idx + p, id);
-        ld<V>(val + p, v);
+    constexpr int kDepth = V >= 4 ? 1 : 4 / V;   // about four entries in flight per lane
+    for (int s0 = 0; s0 < steps; s0 += kDepth * V) {
+        int32_t id[kDepth][V];
+        TV v[kDepth][V];
 #pragma unroll
-        for (int q = 0; q < V; ++q) {
-            const int k = ((s + q) << lp.glog) + lp.g;
-            if (k < len) fetch(acc, static_cast<TA>(v[q]), id[q]);
+        for (int u = 0; u < kDepth; ++u) {
+            const int s = s0 + u * V;
+            if (s < steps) {
+                const int64_t p = base + static_cast<int64_t>(s) * 32 + lane * V;
+                ld<V>(idx + p, id[u]);
+                ld<V>(val + p, v[u]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < V; ++q) {
+                    id[u][q] = 0;
+                    v[u][q] = TV(0);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kDepth; ++u) {
+#pragma unroll
+            for (int q = 0; q < V; ++q) {
+                const int k = ((s0 + u * V + q) << lp.glog) + lp.g;
+                if (k < len) fetch(acc, static_cast<TA>(v[u][q]), id[u][q]);
+            }
         }
     }
     for (int o = (1 << lp.glog) >> 1; o > 0; o >>= 1) {
@@ -190,7 +207,7 @@ template <> __device__ __forceinline__ float min_dual_step<float>() { return 1e-
 // Primal half (pdhg_kernel.cpp:47-104)
 // ---------------------------------------------------------------------------
 template <class T, int V>
-__global__ void __launch_bounds__(kThreads) k_primal(Global g, Work<T> w) {
+__global__ void __launch_bounds__(kThreads, 6) k_primal(Global g, Work<T> w) {
     const CtaWork cw = g.at.ctas[blockIdx.x];
     const InstanceCtl& c = g.ctl[cw.instance];
     if (!g.measure && !trial_active<T>(c)) return;
@@ -216,23 +233,32 @@ __global__ void __launch_bounds__(kThreads) k_primal(Global g, Work<T> w) {
     for (int s = cw.slice_begin + warp; s < cw.slice_end; s += kWarps) {
         const SliceDesc sd = g.at.slices[s];
         const LanePos lp = lane_pos(sd, lane);
-        const int len = lp.valid ? g.at.line_len[inf.at_len_base + lp.line] : 0;
+        const bool owner = lp.valid && lp.g == 0;
+        const int j = lp.line;
+        const int len = lp.valid ? g.at.line_len[inf.at_len_base + j] : 0;
+        // The epilogue's operands do not depend on the product: load them
+        // first so their latency overlaps the gathers.
+        T cj = T(0), prev = T(0), loj = T(0), hij = T(0), tj = T(0), itj = T(0), aj = T(0);
+        if (owner) {
+            cj = cv[j];
+            prev = x[j];
+            loj = lo[j];
+            hij = hi[j];
+            tj = tau[j];
+            itj = itau[j];
+            if (pending) aj = avg[j];
+        }
         T sum[1] = {T(0)};
         line_sums<V, 1>(inf.at_data_base + static_cast<int64_t>(sd.data_off) * 32, sd.steps, lp,
                         lane, len, g.at.idx, vals, sum,
                         [&](T (&a)[1], T v, int i) { a[0] += v * y[i]; });
-        if (lp.valid && lp.g == 0) {
-            const int j = lp.line;
-            const T gradient = cv[j] + sum[0];
-            const T prev = x[j];
-            const T upd = smax(lo[j], smin(prev - mult * tau[j] * gradient, hi[j]));
+        if (owner) {
+            const T gradient = cj + sum[0];
+            const T upd = smax(loj, smin(prev - mult * tj * gradient, hij));
             xt[j] = upd;
             const double d = static_cast<double>(upd - prev);
-            moved[0] += d * d * static_cast<double>(itau[j]);
-            if (pending) {
-                const T a = avg[j];
-                avg[j] = a + frac * (prev - a);
-            }
+            moved[0] += d * d * static_cast<double>(itj);
+            if (pending) avg[j] = aj + frac * (prev - aj);
         }
     }
     block_sum<1>(moved);
@@ -243,7 +269,7 @@ __global__ void __launch_bounds__(kThreads) k_primal(Global g, Work<T> w) {
 // Dual half (pdhg_kernel.cpp:109-187) and the trial decision
 // ---------------------------------------------------------------------------
 template <class T, int V>
-__global__ void __launch_bounds__(kThreads) k_dual(Global g, Work<T> w, DeviceOptions o) {
+__global__ void __launch_bounds__(kThreads, 6) k_dual(Global g, Work<T> w, DeviceOptions o) {
     const CtaWork cw = g.a.ctas[blockIdx.x];
     InstanceCtl& c = g.ctl[cw.instance];
     if (!g.measure && !trial_active<T>(c)) return;
@@ -270,29 +296,36 @@ __global__ void __launch_bounds__(kThreads) k_dual(Global g, Work<T> w, DeviceOp
     for (int s = cw.slice_begin + warp; s < cw.slice_end; s += kWarps) {
         const SliceDesc sd = g.a.slices[s];
         const LanePos lp = lane_pos(sd, lane);
-        const int len = lp.valid ? g.a.line_len[inf.a_len_base + lp.line] : 0;
+        const bool owner = lp.valid && lp.g == 0;
+        const int i = lp.line;
+        const int len = lp.valid ? g.a.line_len[inf.a_len_base + i] : 0;
+        T axi = T(0), sgi = T(0), prev = T(0), loi = T(0), hii = T(0), isi = T(0), ai = T(0);
+        if (owner) {
+            axi = ax[i];
+            sgi = sig[i];
+            prev = y[i];
+            loi = lo[i];
+            hii = hi[i];
+            isi = isig[i];
+            if (pending) ai = avg[i];
+        }
         T sum[1] = {T(0)};
         line_sums<V, 1>(inf.a_data_base + static_cast<int64_t>(sd.data_off) * 32, sd.steps, lp,
                         lane, len, g.a.idx, vals, sum,
                         [&](T (&a)[1], T v, int j) { a[0] += v * xt[j]; });
-        if (lp.valid && lp.g == 0) {
-            const int i = lp.line;
+        if (owner) {
             const T next = sum[0];
-            const T dact = next - ax[i];
+            const T dact = next - axi;
             const T ext = next + dact;
-            const T step = smax(dm * sig[i], min_dual_step<T>());
-            const T prev = y[i];
+            const T step = smax(dm * sgi, min_dual_step<T>());
             const T v = prev + step * ext;
-            const T upd = smax(v - step * hi[i], T(0)) + smin(v - step * lo[i], T(0));
+            const T upd = smax(v - step * hii, T(0)) + smin(v - step * loi, T(0));
             yt[i] = upd;
             axt[i] = next;
             const double d = static_cast<double>(upd - prev);
-            red[0] += d * d * static_cast<double>(isig[i]);
+            red[0] += d * d * static_cast<double>(isi);
             red[1] += d * static_cast<double>(dact);
-            if (pending) {
-                const T a = avg[i];
-                avg[i] = a + frac * (prev - a);
-            }
+            if (pending) avg[i] = ai + frac * (prev - ai);
         }
     }
     block_sum<2>(red);
@@ -438,7 +471,7 @@ __global__ void __launch_bounds__(kThreads) k_check_prep(Global g, Work<T> w, De
 // ---------------------------------------------------------------------------
 // Check, matrix passes and decision
 // ---------------------------------------------------------------------------
-__device__ void check_control(const Global& g, const DeviceOptions& o, InstanceCtl& c,
+__device__ __noinline__ void check_control(const Global& g, const DeviceOptions& o, InstanceCtl& c,
                               const InstanceInfo& inf) {
     // Column-side and row-side elementwise partials.
     double C[kPrepSlots], R[kPrepSlots], A3[3], T6[kCheckSlots];

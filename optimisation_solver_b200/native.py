@@ -111,6 +111,18 @@ SIGNATURES = {
                                          _i32p, _i64p, _dp]),
     "pdlpgpu_session_last_timing": (C.c_int32, [C.c_void_p, _dp, _i64p]),
     "pdlpgpu_session_time_kernels": (C.c_int32, [C.c_void_p, C.c_int32, _dp]),
+    "pdlpgpu_mlp_create": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
+                                       C.c_int32, C.POINTER(C.c_void_p)]),
+    "pdlpgpu_mlp_destroy": (None, [C.c_void_p]),
+    "pdlpgpu_mlp_forward": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pdlpgpu_mlp_train_step": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_float, C.POINTER(C.c_float)]),
+    "pdlpgpu_mlp_gradients": (C.c_int32, [C.c_void_p] + [C.c_void_p] * 9 + [C.POINTER(C.c_float)]),
+    "pdlpgpu_mlp_get_params": (C.c_int32, [C.c_void_p] + [C.c_void_p] * 6),
+    "pdlpgpu_mlp_set_params": (C.c_int32, [C.c_void_p] + [C.c_void_p] * 6),
+    "pdlpgpu_gemm_bf16": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_int32]),
+    "pdlpgpu_mlp_launches": (C.c_int64, [C.c_void_p]),
 }
 
 _LIB = None
