@@ -116,7 +116,8 @@ typedef struct pdlpgpu_ext_options {
     int32_t fp32_stall_checks;     /* mixed: checks without progress before the FP64 stage (0 = 8) */
     int32_t fp32_switch_factor;    /* mixed: FP64 stage once KKT <= factor * tol fails to improve (0 = 1) */
     int32_t disable_graphs;        /* 1: launch kernels directly instead of CUDA graphs */
-    int32_t reserved[8];
+    int32_t cta_slots;             /* SpMV tuning: matrix slots per CTA (0 = autotune) */
+    int32_t reserved[7];
 } pdlpgpu_ext_options;
 
 /* Optional warm start (this engine's extension; the reference starts from the

@@ -63,6 +63,28 @@ int32_t pdlpgpu_mlp_set_params(pdlpgpu_mlp* mlp, const float* W1, const float* b
 int32_t pdlpgpu_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint16_t* A, const uint16_t* B,
                           float* C, int32_t splits);
 
+/* Codec between an LP family's instances and the network (device pointers,
+ * default stream). Features: the instance parameters [batch][count] (FP64)
+ * standardised per feature and rounded to BF16, zero-padded to `padded`
+ * columns. Targets: primal / primal_scale (the flow over its capacity), the
+ * standardised row duals and the standardised log of the final primal
+ * weight, zero-padded to out_width. Decoding inverts the targets and clamps
+ * the primal to [0, primal_scale]; the result feeds pdlpgpu_session_load as
+ * a warm start. Each returns 0 or -1. */
+int32_t pdlpgpu_encode_features(const double* params, int32_t batch, int32_t count,
+                                int32_t padded, const float* mean, const float* inv_std,
+                                uint16_t* out);
+int32_t pdlpgpu_encode_targets(const double* primal, const double* dual, const double* weight,
+                               int32_t batch, int32_t n, int32_t m, int32_t out_width,
+                               const double* primal_scale, const float* dual_mean,
+                               const float* dual_inv_std, float weight_mean,
+                               float weight_inv_std, float* targets);
+int32_t pdlpgpu_decode_warmstart(const float* outputs, int32_t batch, int32_t n, int32_t m,
+                                 int32_t out_width, const double* primal_scale,
+                                 const float* dual_mean, const float* dual_std,
+                                 float weight_mean, float weight_std, double* primal,
+                                 double* dual, double* weight);
+
 /* Kernel launches issued by the last forward / train step of `mlp`. */
 int64_t pdlpgpu_mlp_launches(pdlpgpu_mlp* mlp);
 

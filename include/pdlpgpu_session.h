@@ -49,12 +49,29 @@ int32_t pdlpgpu_session_solve(pdlpgpu_session* session);
 
 /* Results of the last solve. primal [batch][n], dual [batch][m] (original
  * order, device pointers when on_device = 1); per-instance status and
- * iterations on the host; any pointer may be NULL. stats[batch][6] =
+ * iterations on the host; any pointer may be NULL. stats[batch][8] =
  * {primal objective, dual objective, primal residual, dual residual,
- * relative gap, step trials}. Returns 0 on success. */
+ * relative gap, step trials, final primal weight, restarts}. Returns 0 on
+ * success. */
 int32_t pdlpgpu_session_read(pdlpgpu_session* session, int32_t on_device, double* primal,
                              double* dual, int32_t* status, int64_t* iterations,
                              double* stats);
+
+/* Solves `count` instances through the session's `batch` slots, refilling a
+ * slot with the next queued instance as soon as its instance finishes, so a
+ * few slow instances never hold the whole batch. Inputs as for
+ * pdlpgpu_session_load but with `count` rows ([count][n] / [count][m];
+ * warm_weight [count]); outputs primal [count][n], dual [count][m] (device
+ * pointers when on_device = 1, else host), status and iterations [count]
+ * and stats [count][8] (host, as pdlpgpu_session_read). Returns the number
+ * of OPTIMAL instances, or -1 on failure. */
+int32_t pdlpgpu_session_stream(pdlpgpu_session* session, int32_t on_device, int64_t count,
+                               const double* objective, const double* row_lower,
+                               const double* row_upper, const double* var_lower,
+                               const double* var_upper, const double* warm_primal,
+                               const double* warm_dual, const double* warm_weight,
+                               double* primal, double* dual, int32_t* status,
+                               int64_t* iterations, double* stats);
 
 /* Device seconds of the last solve's iteration loop and the number of this
  * library's kernel launches in it. */

@@ -474,6 +474,31 @@ int32_t pdlpgpu_session_read(pdlpgpu_session* s, int32_t on_device, double* prim
     }
 }
 
+int32_t pdlpgpu_session_stream(pdlpgpu_session* s, int32_t on_device, int64_t count,
+                               const double* objective, const double* row_lower,
+                               const double* row_upper, const double* var_lower,
+                               const double* var_upper, const double* warm_primal,
+                               const double* warm_dual, const double* warm_weight,
+                               double* primal, double* dual, int32_t* status, int64_t* iterations,
+                               double* stats) {
+    if (s == nullptr || count < 0) return -1;
+    try {
+        const double* in[5] = {objective, row_lower, row_upper, var_lower, var_upper};
+        if (!s->engine.session_stream(on_device != 0, count, in, warm_primal, warm_dual, warm_weight,
+                                      primal, dual, status, iterations, stats)) {
+            set_error(s->engine.error());
+            return -1;
+        }
+        int32_t optimal = 0;
+        if (status != nullptr)
+            for (int64_t i = 0; i < count; ++i) optimal += status[i] == PDLPGPU_OPTIMAL ? 1 : 0;
+        return optimal;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
 int32_t pdlpgpu_session_last_timing(pdlpgpu_session* s, double* device_seconds, int64_t* launches) {
     if (s == nullptr) return -1;
     if (device_seconds) *device_seconds = s->engine.device_seconds();

@@ -214,8 +214,9 @@ bool Engine::prepare(const SolveSpec& spec) {
         a_slices_ += static_cast<int32_t>(layouts_[k].a.slices.size());
         at_slices_ += static_cast<int32_t>(layouts_[k].at.slices.size());
     }
-    const int64_t target_a = cta_target_slots(spec.shared_matrix ? a_slots_ * count_ : a_slots_, sms_);
-    const int64_t target_at = cta_target_slots(spec.shared_matrix ? at_slots_ * count_ : at_slots_, sms_);
+    int64_t target_a = cta_target_slots(spec.shared_matrix ? a_slots_ * count_ : a_slots_, sms_);
+    int64_t target_at = cta_target_slots(spec.shared_matrix ? at_slots_ * count_ : at_slots_, sms_);
+    if (spec.ext.cta_slots > 0) target_a = target_at = spec.ext.cta_slots;
     a_ctas_.clear();
     at_ctas_.clear();
     vec_.clear();
@@ -1192,9 +1193,10 @@ bool Engine::session_read(bool on_device, double* primal, double* dual, int32_t*
             if (status) status[b] = c.phase == kPhaseDone ? c.status : PDLPGPU_NUMERICAL_FAILURE;
             if (iterations) iterations[b] = c.iteration;
             if (stats) {
-                double* st = stats + 6 * b;
+                double* st = stats + 8 * b;
                 st[0] = c.best_pobj; st[1] = c.best_dobj; st[2] = c.best_pres;
                 st[3] = c.best_dres; st[4] = c.best_gap; st[5] = static_cast<double>(c.step_trials);
+                st[6] = c.omega; st[7] = static_cast<double>(c.restart_count);
             }
         }
     }
@@ -1237,6 +1239,207 @@ bool Engine::time_kernels(int reps, double* out) {
     out[4] = s_at - e_at;
     out[5] = s_a - e_a;
     return true;
+}
+
+
+// ---------------------------------------------------------------------------
+// Streams
+// ---------------------------------------------------------------------------
+bool Engine::ensure_graph() {
+    if (graph_ != nullptr || spec_.ext.disable_graphs) return true;
+    const int slack = spec_.ext.chunk_slack > 0 ? spec_.ext.chunk_slack : 4;
+    const int slots = std::max(1, std::min(spec_.opt.termination_check_frequency + slack, 1024));
+    return build_graph(slots);
+}
+
+bool Engine::session_stream(bool on_device, int64_t N, const double* const in[5], const double* wx,
+                            const double* wy, const double* ww, double* out_x, double* out_y,
+                            int32_t* status, int64_t* iterations, double* stats) {
+    t0_ = std::chrono::steady_clock::now();
+    const int32_t B = count_;
+    const int64_t n = info_[0].n, m = info_[0].m;
+    const pdlpgpu_options& o = spec_.opt;
+    std::vector<void*> temp;   // per-call device buffers
+    auto dalloc = [&](auto*& p, size_t count, std::vector<void*>& list) {
+        void* q = nullptr;
+        if (!check(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(*p)), "cudaMalloc")) return false;
+        list.push_back(q);
+        p = static_cast<std::remove_reference_t<decltype(p)>>(q);
+        return true;
+    };
+    struct Free {
+        std::vector<void*>& v;
+        ~Free() { for (void* q : v) cudaFree(q); }
+    } free_temp{temp};
+    if (d_inst_ == nullptr) {
+        if (!dalloc(d_inst_, B, extra_) || !dalloc(d_mask_, B, extra_) || !dalloc(d_done_, B, extra_) ||
+            !dalloc(d_zero_perm_, 1, extra_))
+            return false;
+        if (!check(cudaMemsetAsync(d_zero_perm_, 0, sizeof(int32_t), stream_), "memset")) return false;
+    }
+    // Inputs and outputs on the device.
+    const int64_t lens[5] = {n, m, m, n, n};
+    const double* src[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    const double *swx = wx, *swy = wy, *sww = ww;
+    double *dox = out_x, *doy = out_y;
+    auto up = [&](const double* h, int64_t count, const double*& d) {
+        double* q = nullptr;
+        if (!dalloc(q, static_cast<size_t>(count), temp)) return false;
+        d = q;
+        return check(cudaMemcpyAsync(q, h, static_cast<size_t>(count) * 8, cudaMemcpyHostToDevice, stream_), "upload");
+    };
+    for (int k = 0; k < 5; ++k) {
+        if (in[k] == nullptr) continue;
+        if (on_device) src[k] = in[k];
+        else if (!up(in[k], N * lens[k], src[k])) return false;
+    }
+    if (!on_device) {
+        if (wx && !up(wx, N * n, swx)) return false;
+        if (wy && !up(wy, N * m, swy)) return false;
+        if (ww && !up(ww, N, sww)) return false;
+        if (out_x && !dalloc(dox, static_cast<size_t>(N * n), temp)) return false;
+        if (out_y && !dalloc(doy, static_cast<size_t>(N * m), temp)) return false;
+    }
+    const bool warm = wx != nullptr || wy != nullptr;
+    if (!ensure_graph()) return false;
+
+    launch_retire(g_, B, stream_);
+    std::vector<int64_t> slot(static_cast<size_t>(B), -1);
+    std::vector<int32_t> mask(static_cast<size_t>(B), 0), done(static_cast<size_t>(B), 0);
+    std::vector<InstanceCtl> ctl(static_cast<size_t>(B));
+    int64_t next = 0;
+    const int slack = spec_.ext.chunk_slack > 0 ? spec_.ext.chunk_slack : 4;
+    const int slots = graph_slots_ > 0 ? graph_slots_ : std::max(1, std::min(o.termination_check_frequency + slack, 1024));
+    const int per_chunk = 2 * slots + (mixed_ ? 8 : 5);
+    launches_ = 0;
+
+    auto upload_slots = [&]() {
+        return check(cudaMemcpyAsync(d_inst_, slot.data(), slot.size() * 8, cudaMemcpyHostToDevice, stream_), "upload") &&
+               check(cudaMemcpyAsync(d_mask_, mask.data(), mask.size() * 4, cudaMemcpyHostToDevice, stream_), "upload");
+    };
+    auto refill = [&]() {
+        bool any = false;
+        for (int32_t b = 0; b < B; ++b) {
+            mask[b] = 0;
+            if (slot[b] < 0 && next < N) {
+                slot[b] = next++;
+                mask[b] = 1;
+                any = true;
+            }
+        }
+        if (!any) return true;
+        if (!upload_slots()) return false;
+        double* dst[5] = {const_cast<double*>(g_.c_orig), const_cast<double*>(g_.rl_orig),
+                          const_cast<double*>(g_.ru_orig), const_cast<double*>(g_.xl_orig),
+                          const_cast<double*>(g_.xu_orig)};
+        for (int k = 0; k < 5; ++k) {
+            const bool cols = k == 0 || k >= 3;
+            launch_gather_slots(src[k], fam_[k], dst[k], cols ? d_col_perm_ : d_row_perm_, d_inst_, d_mask_,
+                                lens[k], B, stream_);
+        }
+        Global gm = g_;
+        gm.slot_mask = d_mask_;
+        gm.warm_x = nullptr;
+        gm.warm_y = nullptr;
+        if (swx) {
+            launch_gather_slots(swx, nullptr, warm_x_, d_col_perm_, d_inst_, d_mask_, n, B, stream_);
+            gm.warm_x = warm_x_;
+        }
+        if (swy) {
+            launch_gather_slots(swy, nullptr, warm_y_, d_row_perm_, d_inst_, d_mask_, m, B, stream_);
+            gm.warm_y = warm_y_;
+        }
+        if (sww) launch_gather_slots(sww, nullptr, warm_w_, d_zero_perm_, d_inst_, d_mask_, 1, B, stream_);
+        launch_norm_parts(gm, stream_);
+        launch_init_ctl(gm, dopt_, B, mixed_ ? 1 : 0, warm ? 1 : 0, sww ? warm_w_ : nullptr,
+                        session_eta_max_, o.initial_primal_weight, family_.objective_offset, stream_);
+        launch_setup_vectors<double>(gm, w64_, stream_);
+        if (mixed_) launch_setup_vectors<float>(gm, w32_, stream_);
+        const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
+        (void)elapsed;
+        launch_stamp_clock(gm, B, 0, o.time_limit_seconds > 0.0 ? static_cast<int64_t>(o.time_limit_seconds * 1e9) : 0,
+                           stream_);
+        if (mixed_) launch_refresh<float>(g_, w32_, dopt_, tuning_.vector_width, stream_);
+        launch_refresh<double>(g_, w64_, dopt_, tuning_.vector_width, stream_);
+        enqueue_check_stage();
+        launches_ += 12;
+        return check(cudaGetLastError(), "refill");
+    };
+    auto harvest = [&]() {
+        bool any = false;
+        for (int32_t b = 0; b < B; ++b) {
+            mask[b] = (done[b] && slot[b] >= 0) ? 1 : 0;
+            any = any || mask[b];
+        }
+        if (!any) return true;
+        if (!upload_slots()) return false;
+        if (dox) launch_scatter_slots(g_.best_x, dox, d_col_perm_, d_inst_, d_mask_, n, B, stream_);
+        if (doy) launch_scatter_slots(g_.best_y, doy, d_row_perm_, d_inst_, d_mask_, m, B, stream_);
+        if (!check(cudaMemcpyAsync(ctl.data(), g_.ctl, ctl.size() * sizeof(InstanceCtl), cudaMemcpyDeviceToHost, stream_), "download") ||
+            !check(cudaStreamSynchronize(stream_), "harvest"))
+            return false;
+        for (int32_t b = 0; b < B; ++b) {
+            if (!mask[b]) continue;
+            const InstanceCtl& c = ctl[static_cast<size_t>(b)];
+            const int64_t i = slot[b];
+            if (status) status[i] = c.status;
+            if (iterations) iterations[i] = c.iteration;
+            if (stats) {
+                double* st = stats + 8 * i;
+                st[0] = c.best_pobj; st[1] = c.best_dobj; st[2] = c.best_pres; st[3] = c.best_dres;
+                st[4] = c.best_gap; st[5] = static_cast<double>(c.step_trials); st[6] = c.omega;
+                st[7] = static_cast<double>(c.restart_count);
+            }
+            slot[b] = -1;
+        }
+        return true;
+    };
+
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, stream_);
+    bool ok = refill();
+    const int64_t trials_bound =
+        (std::max<int64_t>(o.iteration_limit, 0) + std::max(o.polishing_iterations, 0) + 2) *
+        std::max(o.maximum_step_trials, 1);
+    const int64_t max_chunks = (trials_bound / std::max(1, slots - slack) + 64) * ((N + B - 1) / B + 1);
+    int64_t chunks = 0;
+    while (ok) {
+        launch_slot_done(g_, B, d_done_, stream_);
+        ok = check(cudaMemcpyAsync(done.data(), d_done_, done.size() * 4, cudaMemcpyDeviceToHost, stream_), "poll") &&
+             check(cudaStreamSynchronize(stream_), "poll");
+        if (!ok) break;
+        ok = harvest() && refill();
+        if (!ok) break;
+        bool active = false;
+        for (int32_t b = 0; b < B; ++b) active = active || slot[b] >= 0;
+        if (!active && next >= N) break;
+        if (++chunks > max_chunks) {
+            error_ = "stream exceeded its chunk bound";
+            ok = false;
+            break;
+        }
+        if (graph_) {
+            ok = check(cudaGraphLaunch(graph_, stream_), "graph launch");
+            launches_ += per_chunk;
+        } else {
+            enqueue_chunk(slots);
+        }
+    }
+    cudaEventRecord(e1, stream_);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    device_seconds_ = 1e-3 * ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ok && !on_device) {
+        if (out_x) ok = check(cudaMemcpyAsync(out_x, dox, static_cast<size_t>(N * n) * 8, cudaMemcpyDeviceToHost, stream_), "download");
+        if (ok && out_y) ok = check(cudaMemcpyAsync(out_y, doy, static_cast<size_t>(N * m) * 8, cudaMemcpyDeviceToHost, stream_), "download");
+        ok = ok && check(cudaStreamSynchronize(stream_), "download");
+    }
+    return ok;
 }
 
 }  // namespace pdlpgpu

@@ -57,6 +57,11 @@ public:
     bool session_read(bool on_device, double* primal, double* dual, int32_t* status,
                       int64_t* iterations, double* stats);
     bool time_kernels(int reps, double* out);
+    // Solves N instances through the session's slots, refilling each slot with
+    // the next instance as soon as its instance finishes.
+    bool session_stream(bool on_device, int64_t N, const double* const in[5], const double* wx,
+                        const double* wy, const double* ww, double* out_x, double* out_y,
+                        int32_t* status, int64_t* iterations, double* stats);
     int32_t count() const { return count_; }
 
     // --- component tests (single instance, internal order handled here) ---
@@ -77,6 +82,7 @@ private:
     void enqueue_check_stage();
     bool check(cudaError_t e, const char* what);
     bool build_graph(int slots);
+    bool ensure_graph();
     bool power_iteration();
     bool setup_kernels();
     bool init_control();
@@ -137,6 +143,10 @@ private:
     bool session_warm_ = false;
     bool session_has_ww_ = false;
     double session_eta_max_ = 0.99;
+    int64_t* d_inst_ = nullptr;       // stream: instance in each slot
+    int32_t* d_mask_ = nullptr;       // stream: slots being refilled / harvested
+    int32_t* d_done_ = nullptr;       // stream: finished flags
+    int32_t* d_zero_perm_ = nullptr;  // {0}: identity permutation of length 1
     pdlpgpu_lp family_{};
 };
 

@@ -983,6 +983,7 @@ __device__ __forceinline__ double initial_value(double lo, double hi) {   // pdl
 template <class T>
 __global__ void k_setup_vectors(Global g, Work<T> w) {
     const VecWork vw = g.vec[blockIdx.x];
+    if (g.slot_mask != nullptr && g.slot_mask[vw.instance] == 0) return;
     const InstanceInfo inf = g.info[vw.instance];
     const bool warm = g.warm_x != nullptr || g.warm_y != nullptr;
     if (!vw.is_row) {
@@ -1169,6 +1170,7 @@ __global__ void k_power_finish(Global g, int32_t count, double safety, double mi
 __global__ void k_stamp_clock(Global g, int32_t count, int64_t elapsed_ns, int64_t limit_ns) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= count) return;
+    if (g.slot_mask != nullptr && g.slot_mask[b] == 0) return;
     InstanceCtl& c = g.ctl[b];
     c.start_ns = now_ns() - elapsed_ns;
     c.deadline_ns = limit_ns > 0 ? c.start_ns + limit_ns : 0;
@@ -1194,6 +1196,7 @@ __global__ void k_permute(const double* __restrict__ src, double* __restrict__ d
 
 __global__ void __launch_bounds__(kThreads) k_norm_parts(Global g) {
     const VecWork vw = g.vec[blockIdx.x];
+    if (g.slot_mask != nullptr && g.slot_mask[vw.instance] == 0) return;
     const InstanceInfo inf = g.info[vw.instance];
     double acc[1] = {0.0};
     if (!vw.is_row) {
@@ -1218,6 +1221,7 @@ __global__ void k_init_ctl(Global g, DeviceOptions o, int32_t count, int32_t mix
                            double objective_offset) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= count) return;
+    if (g.slot_mask != nullptr && g.slot_mask[b] == 0) return;
     const InstanceInfo inf = g.info[b];
     double rows = 0.0, cols = 0.0;
     for (int k = inf.vec_cta_begin; k < inf.vec_cta_end; ++k) {
@@ -1250,6 +1254,50 @@ __global__ void k_init_ctl(Global g, DeviceOptions o, int32_t count, int32_t mix
     c.dnorm = 1.0 + sqrt(cols);
     c.objective_offset = objective_offset;
     g.ctl[b] = c;
+}
+
+
+// ---------------------------------------------------------------------------
+// Streams: refill finished slots with the next instances of a queue.
+// ---------------------------------------------------------------------------
+__global__ void k_gather_slots(const double* __restrict__ src, const double* __restrict__ fam,
+                               double* __restrict__ dst, const int32_t* __restrict__ perm,
+                               const int64_t* __restrict__ inst, const int32_t* __restrict__ mask,
+                               int64_t len, int32_t count) {
+    const int64_t total = len * count;
+    for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t b = t / len, k = t - b * len;
+        if (mask[b] == 0) continue;
+        dst[t] = src != nullptr ? src[inst[b] * len + perm[k]] : fam[k];
+    }
+}
+
+__global__ void k_scatter_slots(const double* __restrict__ src, double* __restrict__ out,
+                                const int32_t* __restrict__ perm, const int64_t* __restrict__ inst,
+                                const int32_t* __restrict__ mask, int64_t len, int32_t count) {
+    const int64_t total = len * count;
+    for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t b = t / len, k = t - b * len;
+        if (mask[b] == 0) continue;
+        out[inst[b] * len + perm[k]] = src[t];
+    }
+}
+
+// Marks every slot finished (no work) before a stream fills them.
+__global__ void k_retire(Global g, int32_t count) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= count) return;
+    InstanceCtl& c = g.ctl[b];
+    c.phase = kPhaseDone;
+    c.stage = kStageTrial;
+    c.best_src = c.restart_src = c.need_refresh = c.to_polish = c.save_ray = 0;
+}
+
+__global__ void k_slot_done(Global g, int32_t count, int32_t* done) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < count) done[b] = g.ctl[b].phase == kPhaseDone ? 1 : 0;
 }
 
 inline unsigned blocks_for(int64_t n, int per) { return static_cast<unsigned>((n + per - 1) / per); }
@@ -1420,6 +1468,28 @@ void launch_init_ctl(const Global& g, const DeviceOptions& o, int32_t count, int
     if (count)
         k_init_ctl<<<blocks_for(count, 128), 128, 0, s>>>(g, o, count, mixed, warm, warm_weight,
                                                           eta_max, initial_weight, objective_offset);
+}
+
+void launch_gather_slots(const double* src, const double* fam, double* dst, const int32_t* perm,
+                         const int64_t* inst, const int32_t* mask, int64_t len, int32_t count,
+                         cudaStream_t s) {
+    const int64_t total = len * count;
+    if (total == 0) return;
+    const unsigned blocks = static_cast<unsigned>(std::min<int64_t>((total + 255) / 256, 148 * 16));
+    k_gather_slots<<<blocks, 256, 0, s>>>(src, fam, dst, perm, inst, mask, len, count);
+}
+void launch_scatter_slots(const double* src, double* out, const int32_t* perm, const int64_t* inst,
+                          const int32_t* mask, int64_t len, int32_t count, cudaStream_t s) {
+    const int64_t total = len * count;
+    if (total == 0) return;
+    const unsigned blocks = static_cast<unsigned>(std::min<int64_t>((total + 255) / 256, 148 * 16));
+    k_scatter_slots<<<blocks, 256, 0, s>>>(src, out, perm, inst, mask, len, count);
+}
+void launch_retire(const Global& g, int32_t count, cudaStream_t s) {
+    if (count) k_retire<<<blocks_for(count, 128), 128, 0, s>>>(g, count);
+}
+void launch_slot_done(const Global& g, int32_t count, int32_t* done, cudaStream_t s) {
+    if (count) k_slot_done<<<blocks_for(count, 128), 128, 0, s>>>(g, count, done);
 }
 
 #define PDLPGPU_INSTANTIATE(T)                                                                      \

@@ -83,6 +83,8 @@ struct Global {
     // 1: timing mode -- every instance runs its trial kernels, no decision is
     // taken and no state changes (the trial buffers are scratch).
     int32_t measure;
+    // Streams: when set, setup kernels act only on slots with slot_mask[b] != 0.
+    const int32_t* slot_mask;
 };
 
 // --- launches (kernels.cu). `vw` is the vector width (1, 2 or 4). ---------
@@ -137,6 +139,15 @@ void launch_stamp_clock(const Global& g, int32_t count, int64_t elapsed_ns, int6
 void launch_permute(const double* src, double* dst, const int32_t* perm, int64_t len,
                     int32_t count, int mode, cudaStream_t s);
 void launch_norm_parts(const Global& g, cudaStream_t s);
+// Streams: per slot b with mask[b] != 0, dst[b][k] = src[inst[b]][perm[k]]
+// (src = null: fam[k]); scatter: out[inst[b]][perm[k]] = src[b][k].
+void launch_gather_slots(const double* src, const double* fam, double* dst, const int32_t* perm,
+                         const int64_t* inst, const int32_t* mask, int64_t len, int32_t count,
+                         cudaStream_t s);
+void launch_scatter_slots(const double* src, double* out, const int32_t* perm, const int64_t* inst,
+                          const int32_t* mask, int64_t len, int32_t count, cudaStream_t s);
+void launch_retire(const Global& g, int32_t count, cudaStream_t s);
+void launch_slot_done(const Global& g, int32_t count, int32_t* done, cudaStream_t s);
 void launch_init_ctl(const Global& g, const DeviceOptions& o, int32_t count, int32_t mixed,
                      int32_t warm, const double* warm_weight, double eta_max,
                      double initial_weight, double objective_offset, cudaStream_t s);

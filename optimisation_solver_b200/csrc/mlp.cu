@@ -369,6 +369,55 @@ __global__ void to_bf16(const float* src, bf16* dst, int64_t n) {
         dst[t] = __float2bfloat16_rn(src[t]);
 }
 
+// --- codec between LP instances and the network -----------------------------
+// Features: standardised instance parameters, BF16, zero-padded to `padded`.
+__global__ void encode_features(const double* params, int B, int P, int padded, const float* mean,
+                                const float* inv_std, bf16* out) {
+    const int64_t total = static_cast<int64_t>(B) * padded;
+    for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t b = t / padded;
+        const int k = static_cast<int>(t - b * padded);
+        float v = 0.0f;
+        if (k < P) v = (static_cast<float>(params[b * P + k]) - mean[k]) * inv_std[k];
+        out[t] = __float2bfloat16_rn(v);
+    }
+}
+
+// Targets: primal / scale, standardised dual, standardised log weight, zeros.
+__global__ void encode_targets(const double* x, const double* y, const double* w, int B, int n, int m,
+                               int O, const double* scale, const float* ymean, const float* yinv,
+                               float wmean, float winv, float* out) {
+    const int64_t total = static_cast<int64_t>(B) * O;
+    for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t b = t / O;
+        const int j = static_cast<int>(t - b * O);
+        float v = 0.0f;
+        if (j < n) v = static_cast<float>(x[b * n + j] / scale[j]);
+        else if (j < n + m) v = (static_cast<float>(y[b * m + (j - n)]) - ymean[j - n]) * yinv[j - n];
+        else if (j == n + m) v = (logf(static_cast<float>(w[b])) - wmean) * winv;
+        out[t] = v;
+    }
+}
+
+// Warm start from network outputs: x = clamp(out, 0, 1) * scale, y and the
+// weight de-standardised.
+__global__ void decode_warmstart(const float* out, int B, int n, int m, int O, const double* scale,
+                                 const float* ymean, const float* ystd, float wmean, float wstd,
+                                 double* wx, double* wy, double* ww) {
+    const int64_t total = static_cast<int64_t>(B) * (n + m + 1);
+    for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t b = t / (n + m + 1);
+        const int j = static_cast<int>(t - b * (n + m + 1));
+        const float v = out[b * O + j];
+        if (j < n) wx[b * n + j] = static_cast<double>(fminf(fmaxf(v, 0.0f), 1.0f)) * scale[j];
+        else if (j < n + m) wy[b * m + (j - n)] = static_cast<double>(v * ystd[j - n] + ymean[j - n]);
+        else ww[b] = static_cast<double>(expf(v * wstd + wmean));
+    }
+}
+
 inline unsigned grid_for(int64_t n) {
     const int64_t b = (n + 255) / 256;
     return static_cast<unsigned>(b < 148 * 32 ? (b > 0 ? b : 1) : 148 * 32);
@@ -791,6 +840,38 @@ int32_t pdlpgpu_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint16_t* A, co
     cudaFree(err);
     if (partial) cudaFree(partial);
     return ok ? 0 : fail("gemm: " + (msg.empty() ? std::string(cudaGetErrorString(cudaGetLastError())) : msg));
+}
+
+
+int32_t pdlpgpu_encode_features(const double* params, int32_t batch, int32_t count, int32_t padded,
+                                const float* mean, const float* inv_std, uint16_t* out) {
+    if (batch <= 0 || count <= 0 || padded < count) return fail("encode_features: bad sizes");
+    encode_features<<<grid_for(static_cast<int64_t>(batch) * padded), 256>>>(
+        params, batch, count, padded, mean, inv_std, reinterpret_cast<bf16*>(out));
+    return cudaGetLastError() == cudaSuccess ? 0 : fail("encode_features: launch failed");
+}
+
+int32_t pdlpgpu_encode_targets(const double* primal, const double* dual, const double* weight,
+                               int32_t batch, int32_t n, int32_t m, int32_t out_width,
+                               const double* primal_scale, const float* dual_mean,
+                               const float* dual_inv_std, float weight_mean, float weight_inv_std,
+                               float* targets) {
+    if (batch <= 0 || out_width < n + m + 1) return fail("encode_targets: bad sizes");
+    encode_targets<<<grid_for(static_cast<int64_t>(batch) * out_width), 256>>>(
+        primal, dual, weight, batch, n, m, out_width, primal_scale, dual_mean, dual_inv_std,
+        weight_mean, weight_inv_std, targets);
+    return cudaGetLastError() == cudaSuccess ? 0 : fail("encode_targets: launch failed");
+}
+
+int32_t pdlpgpu_decode_warmstart(const float* outputs, int32_t batch, int32_t n, int32_t m,
+                                 int32_t out_width, const double* primal_scale,
+                                 const float* dual_mean, const float* dual_std, float weight_mean,
+                                 float weight_std, double* primal, double* dual, double* weight) {
+    if (batch <= 0 || out_width < n + m + 1) return fail("decode_warmstart: bad sizes");
+    decode_warmstart<<<grid_for(static_cast<int64_t>(batch) * (n + m + 1)), 256>>>(
+        outputs, batch, n, m, out_width, primal_scale, dual_mean, dual_std, weight_mean, weight_std,
+        primal, dual, weight);
+    return cudaGetLastError() == cudaSuccess ? 0 : fail("decode_warmstart: launch failed");
 }
 
 }  // extern "C"

@@ -56,7 +56,8 @@ class ExtOptions(C.Structure):
     _fields_ = [("precision", C.c_int32), ("device", C.c_int32), ("lane_elements", C.c_int32),
                 ("vector_width", C.c_int32), ("chunk_slack", C.c_int32),
                 ("fp32_stall_checks", C.c_int32), ("fp32_switch_factor", C.c_int32),
-                ("disable_graphs", C.c_int32), ("reserved", C.c_int32 * 8)]
+                ("disable_graphs", C.c_int32), ("cta_slots", C.c_int32),
+                ("reserved", C.c_int32 * 7)]
 
 
 class WarmStart(C.Structure):
@@ -110,6 +111,8 @@ SIGNATURES = {
     "pdlpgpu_session_read": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
                                          _i32p, _i64p, _dp]),
     "pdlpgpu_session_last_timing": (C.c_int32, [C.c_void_p, _dp, _i64p]),
+    "pdlpgpu_session_stream": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64] + [C.c_void_p] * 10 +
+                               [_i32p, _i64p, _dp]),
     "pdlpgpu_session_time_kernels": (C.c_int32, [C.c_void_p, C.c_int32, _dp]),
     "pdlpgpu_mlp_create": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
                                        C.c_int32, C.POINTER(C.c_void_p)]),
@@ -123,6 +126,15 @@ SIGNATURES = {
     "pdlpgpu_gemm_bf16": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_int32]),
     "pdlpgpu_mlp_launches": (C.c_int64, [C.c_void_p]),
+    "pdlpgpu_encode_features": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                            C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pdlpgpu_encode_targets": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                           C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_float, C.c_float, C.c_void_p]),
+    "pdlpgpu_decode_warmstart": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                             C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_float, C.c_float, C.c_void_p, C.c_void_p,
+                                             C.c_void_p]),
 }
 
 _LIB = None

@@ -84,7 +84,7 @@ class Session:
                 dual = np.zeros((self.batch, self.m))
         status = np.zeros(self.batch, dtype=np.int32)
         iters = np.zeros(self.batch, dtype=np.int64)
-        stats = np.zeros((self.batch, 6))
+        stats = np.zeros((self.batch, 8))
         rc = native.lib().pdlpgpu_session_read(self._s, int(on_device), _addr(primal), _addr(dual),
                                                native.ptr(status, C.c_int32),
                                                native.ptr(iters, C.c_int64), native.ptr(stats))
@@ -93,7 +93,38 @@ class Session:
         return dict(primal=primal, dual=dual, status=[PdlpStatus(int(s)) for s in status],
                     iterations=iters, primal_objective=stats[:, 0], dual_objective=stats[:, 1],
                     primal_residual=stats[:, 2], dual_residual=stats[:, 3],
-                    relative_gap=stats[:, 4], step_trials=stats[:, 5].astype(np.int64))
+                    relative_gap=stats[:, 4], step_trials=stats[:, 5].astype(np.int64),
+                    final_primal_weight=stats[:, 6], restart_count=stats[:, 7].astype(np.int64))
+
+    def stream(self, count: int, objective=None, row_lower=None, row_upper=None, var_lower=None,
+               var_upper=None, warm_primal=None, warm_dual=None, warm_weight=None, primal=None,
+               dual=None, on_device: bool = False):
+        """Solves `count` instances through the session's slots with refill.
+        Host mode allocates primal/dual outputs when not given; device mode
+        writes into the given device buffers (or none)."""
+        arrs = [objective, row_lower, row_upper, var_lower, var_upper, warm_primal, warm_dual,
+                warm_weight]
+        if not on_device:
+            arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
+            if primal is None:
+                primal = np.zeros((count, self.n))
+            if dual is None:
+                dual = np.zeros((count, self.m))
+        status = np.zeros(count, dtype=np.int32)
+        iters = np.zeros(count, dtype=np.int64)
+        stats = np.zeros((count, 8))
+        k = native.lib().pdlpgpu_session_stream(self._s, int(on_device), int(count),
+                                                *[_addr(a) for a in arrs], _addr(primal),
+                                                _addr(dual), native.ptr(status, C.c_int32),
+                                                native.ptr(iters, C.c_int64), native.ptr(stats))
+        if k < 0:
+            raise RuntimeError(f"session_stream failed: {native.last_error()}")
+        return dict(optimal=k, primal=primal, dual=dual,
+                    status=[PdlpStatus(int(s)) for s in status], iterations=iters,
+                    primal_objective=stats[:, 0], dual_objective=stats[:, 1],
+                    primal_residual=stats[:, 2], dual_residual=stats[:, 3],
+                    relative_gap=stats[:, 4], step_trials=stats[:, 5].astype(np.int64),
+                    final_primal_weight=stats[:, 6], restart_count=stats[:, 7].astype(np.int64))
 
     def last_timing(self):
         s, n = C.c_double(), C.c_int64()
