@@ -1,19 +1,26 @@
 #!/usr/bin/env python
 """Headline benchmark: LPs solved per second at 1e-4 relative KKT on the
 min-cost network-flow family (2000 nodes, 20,000 arcs, one shared incidence
-matrix; per instance random supplies and costs), 256 instances per batched
-device solve, mixed precision (FP32 iterations, FP64 checks).
+matrix; per instance random supplies and costs), learned warm start plus
+batched mixed-precision PDLP, 256 instances per step through 256 device
+slots.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One step = one batch of `batch` LPs solved to the tolerance. `value` is the
-whole-job throughput with the step inputs already resident in HBM; `e2e` is
-the same through the C ABI from pinned host buffers with the solutions read
-back to the host every step. Under torchrun every rank solves its own
-batches (weak scaling, no collective in the loop); the timed region is
-bracketed by a barrier and a device synchronize, and the time is the max over
-ranks. The reference arm times the reference's own CPU PDLP (the library
-oracle/Makefile builds from the reference sources) on the host cores.
+Before the timed region the learned warm start is trained: seeded training
+instances of the family are solved by the engine itself (cold start) and the
+3-layer BF16 MLP is fitted on their solutions with the library's tensor-core
+kernels. One step = 256 fresh instances: their warm starts are predicted on
+the device and they are solved to the tolerance. The timed region holds all
+K steps -- K x 256 predictions, and one stream of K x 256 instances through
+the session's slots (a slot is refilled as soon as its instance ends).
+`value` has the step inputs resident in HBM; `e2e` is the same from pinned
+host buffers, with the solutions copied back to the host. Under torchrun
+every rank solves its own instances (weak scaling, no collective in the
+loop); the timed region is bracketed by a barrier and a device synchronize,
+and the time is the max over ranks. The reference arm times the reference's
+own CPU PDLP (the library oracle/Makefile builds from the reference sources)
+on the host cores.
 """
 from __future__ import annotations
 
@@ -30,8 +37,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "LPs solved/s at 1e-4 rel. KKT (min-cost flow family, batched)"
+METRIC = "LPs solved/s at 1e-4 rel. KKT (min-cost flow family, learned warm start + batched)"
 FALLBACK_HBM_GBS = 6650.0
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "il_trial_kernels_flow_batch256.md")
 
 
 def parse_args():
@@ -40,14 +48,21 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--batch", type=int, default=256)
+    p.add_argument("--batch", type=int, default=256, help="instances per step")
+    p.add_argument("--slots", type=int, default=256, help="device slots of the session")
     p.add_argument("--tol", type=float, default=1e-4)
     p.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    p.add_argument("--cold", action="store_true", help="no learned warm start in the timed path")
+    p.add_argument("--train", type=int, default=20000, help="training instances of the warm start")
+    p.add_argument("--train-tol", type=float, default=1e-4, help="tolerance of the training labels")
+    p.add_argument("--train-precision", choices=["mixed", "fp64"], default="mixed")
+    p.add_argument("--epochs", type=int, default=30)
     p.add_argument("--cpu-sample", type=int, default=32, help="instances in the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--no-extras", action="store_true", help="skip the plain-GPU and large-LP side measurements")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the cold-start, plain-GPU and large-LP side measurements")
     p.add_argument("--profile", action="store_true",
-                   help="load one batch and launch only the timed trial kernels (for ncu captures)")
+                   help="a short cold stream only (for ncu captures of the trial kernels)")
     return p.parse_args()
 
 
@@ -62,10 +77,9 @@ def peaks():
 
 def ncu_traffic(kernel: str):
     """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", "pdhg_kernels_flow_batch256.md")
-    if not os.path.exists(path):
+    if not os.path.exists(PROFILE_SUMMARY):
         return None
-    for line in open(path):
+    for line in open(PROFILE_SUMMARY):
         if line.startswith(f"traffic_bytes_per_launch[{kernel}]:"):
             return float(line.split(":", 1)[1].strip())
     return None
@@ -127,18 +141,16 @@ class ClockSampler:
 
 
 def workload(batch: int, steps: int, rank: int, graph):
+    """Per-step (supply, cost) of fresh instances, seeded per rank and step
+    (disjoint from the training seeds)."""
     from optimisation_solver_b200 import generators as g
-    out = []
-    for k in range(steps):
-        supply, cost = g.flow_parameters(graph, batch, seed=100_000 * (rank + 1) + k)
-        out.append((supply, cost))
-    return out
+    return [g.flow_parameters(graph, batch, seed=100_000 * (rank + 1) + k) for k in range(steps)]
 
 
 def cpu_solve_sample(lib_kind: str, graph, supply, cost, tol: float, threads: int):
     """Solves each (supply, cost) instance with the CPU library, instance
     parallel over `threads` host threads (one solver thread each). Returns
-    (seconds, statuses)."""
+    (seconds, statuses, objectives)."""
     from concurrent.futures import ThreadPoolExecutor
 
     from oracle.oracle import Oracle
@@ -149,7 +161,20 @@ def cpu_solve_sample(lib_kind: str, graph, supply, cost, tol: float, threads: in
     t0 = time.perf_counter()
     with ThreadPoolExecutor(max_workers=threads) as ex:
         res = list(ex.map(lambda lp: orc.solve(lp, opts), lps))
-    return time.perf_counter() - t0, [r.status for r in res]
+    return time.perf_counter() - t0, [r.status for r in res], [r.primal_objective for r in res]
+
+
+def trial_bytes(n, m, nnz, slots, s, family_bounds_x=True):
+    """Algorithmic bytes of one launch of each interleaved trial kernel in the
+    loop (every slot active, average update owed): per instance the line's
+    own vectors once and the gathered vector once; once per launch the
+    matrix (value, index, line pointer) and the broadcast vectors."""
+    primal = (slots * n * s * 5            # x read, c read, average read+write, x' written
+              + n * s * (2 + (2 if family_bounds_x else 0))   # tau, 1/tau, family bounds
+              + nnz * (s + 4) + (n + 1) * 8 + slots * m * s)  # matrix, y gathered
+    dual = (slots * m * s * 8              # Ax, y, row bounds (2), y', Ax', average read+write
+            + m * s * 2 + nnz * (s + 4) + (m + 1) * 8 + slots * n * s)  # sigma, 1/sigma, matrix, x'
+    return primal, dual
 
 
 def main():
@@ -162,9 +187,11 @@ def main():
     from optimisation_solver_b200 import generators as g
     graph = g.flow_graph()
     config = {"workload": "min-cost flow family: 2000 nodes, 20000 arcs, 40000 nnz; "
-                          f"batch {args.batch} per step; tolerance {args.tol:g} relative KKT",
-              "batch": args.batch, "nodes": graph.nodes, "arcs": graph.arcs,
-              "tolerance": args.tol, "l2": "working set > L2 (126 MB) every step"}
+                          f"{args.batch} instances per step through {args.slots} device slots; "
+                          f"tolerance {args.tol:g} relative KKT",
+              "batch": args.batch, "slots": args.slots, "nodes": graph.nodes, "arcs": graph.arcs,
+              "tolerance": args.tol, "warm_start": "cold" if args.cold else "learned",
+              "l2": "working set > L2 (126 MB): 256 x 20000 x 4 B per vector, six vectors per trial"}
 
     if args.impl == "reference":
         return reference_arm(args, world, rank, graph, config)
@@ -181,43 +208,70 @@ def main():
 
     family = g.flow_lp(graph, *[a[0] for a in g.flow_parameters(graph, 1, seed=7)])
     options = PdlpOptions().with_tolerance(args.tol)
-    session = Session(family, args.batch, options, precision=args.precision, device=local_rank)
-
-    steps_in = workload(args.batch, args.warmup + args.steps, rank, graph)
-    # Inputs resident in HBM before the timed region.
-    dev_in = [(torch.from_numpy(s).to(dev), torch.from_numpy(c).to(dev)) for s, c in steps_in]
+    session = Session(family, args.slots, options, precision=args.precision, device=local_rank)
+    n, m, nnz = graph.arcs, graph.nodes, family.nnz
+    K, W, B = args.steps, args.warmup, args.batch
+    steps_in = workload(B, W + K, rank, graph)
+    sup_all = torch.from_numpy(np.concatenate([s for s, _ in steps_in])).to(dev)
+    cost_all = torch.from_numpy(np.concatenate([c for _, c in steps_in])).to(dev)
     torch.cuda.synchronize()
 
-    def step(k):
-        sup, cost = dev_in[k]
-        session.load(objective=cost.data_ptr(), row_lower=sup.data_ptr(), row_upper=sup.data_ptr(),
-                     on_device=True)
-        return session.solve()
-
     if args.profile:
-        sup, cost = dev_in[0]
-        session.load(objective=cost.data_ptr(), row_lower=sup.data_ptr(), row_upper=sup.data_ptr(),
-                     on_device=True)
-        step(0)
-        tk = session.time_kernels(3)
-        print(json.dumps({"profile": tk}))
+        out = session.stream(B, objective=cost_all[:B].data_ptr(), row_lower=sup_all[:B].data_ptr(),
+                             row_upper=sup_all[:B].data_ptr(), on_device=True)
+        print(json.dumps({"profile": session.loop_timing(), "optimal": out["optimal"]}, default=float))
         session.close()
         return
-    for k in range(args.warmup):
-        step(k)
-    launches = 0
-    optimal = 0
+
+    model, train_info = None, None
+    if not args.cold:
+        from optimisation_solver_b200.learned import train_flow_model
+        model, train_info = train_flow_model(graph, args.train, tol=args.train_tol,
+                                             precision=args.train_precision, device=local_rank,
+                                             epochs=args.epochs)
+
+    px = torch.empty((K * B, n), dtype=torch.float64, device=dev)
+    py = torch.empty((K * B, m), dtype=torch.float64, device=dev)
+
+    def predict(sup, cost):
+        """Warm starts for the rows of sup/cost, 256 per network pass."""
+        if model is None:
+            return None, None, None, 0
+        count = sup.shape[0]
+        wx = torch.empty((count, n), dtype=torch.float64, device=dev)
+        wy = torch.empty((count, m), dtype=torch.float64, device=dev)
+        ww = torch.empty((count,), dtype=torch.float64, device=dev)
+        launches = 0
+        for b0 in range(0, count, model.batch):
+            b1 = b0 + model.batch
+            x, y, w = model.predict(sup[b0:b1], cost[b0:b1])
+            wx[b0:b1], wy[b0:b1], ww[b0:b1] = x, y, w
+            launches += 2 + model.mlp.launches()
+        return wx, wy, ww, launches
+
+    def solve(sup, cost, outx=None, outy=None, warm=True):
+        wx, wy, ww, launches = predict(sup, cost) if warm else (None, None, None, 0)
+        ptr = lambda t: None if t is None else t.data_ptr()
+        res = session.stream(sup.shape[0], objective=ptr(cost), row_lower=ptr(sup), row_upper=ptr(sup),
+                             warm_primal=ptr(wx), warm_dual=ptr(wy), warm_weight=ptr(ww),
+                             primal=ptr(outx), dual=ptr(outy), on_device=True)
+        return res, launches + session.last_timing()[1]
+
+    # Warm-up: the first W steps, each solved on its own.
+    for k in range(W):
+        solve(sup_all[k * B:(k + 1) * B], cost_all[k * B:(k + 1) * B])
+
+    timed = slice(W * B, (W + K) * B)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local_rank) as clocks:
         start.record()
-        for k in range(args.warmup, args.warmup + args.steps):
-            optimal += step(k)
-            launches += session.last_timing()[1]
+        res, launches = solve(sup_all[timed], cost_all[timed], px, py)
         end.record()
         torch.cuda.synchronize()
+    loop = session.loop_timing()
     if world > 1:
         dist.barrier()
     elapsed = start.elapsed_time(end) / 1e3
@@ -225,69 +279,106 @@ def main():
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     elapsed_max = float(t.item())
-    value = world * args.batch * args.steps / elapsed_max
+    value = world * K * B / elapsed_max
+    optimal = res["optimal"]
+    iters = res["iterations"]
 
-    # End to end through the C ABI: pinned host inputs copied in, solutions read back.
-    pinned = [(torch.from_numpy(s).pin_memory(), torch.from_numpy(c).pin_memory()) for s, c in steps_in]
-    out_x = torch.empty((args.batch, graph.arcs), dtype=torch.float64).pin_memory()
-    out_y = torch.empty((args.batch, graph.nodes), dtype=torch.float64).pin_memory()
-    h2d = args.batch * (graph.arcs + 2 * graph.nodes) * 8
-    d2h = args.batch * (graph.arcs + graph.nodes) * 8
+    # End to end: pinned host inputs copied in, warm starts predicted, the
+    # stream solved, the solutions copied back to pinned host memory.
+    sup_h = torch.from_numpy(np.concatenate([s for s, _ in steps_in[W:]])).pin_memory()
+    cost_h = torch.from_numpy(np.concatenate([c for _, c in steps_in[W:]])).pin_memory()
+    out_xh = torch.empty((K * B, n), dtype=torch.float64).pin_memory()
+    out_yh = torch.empty((K * B, m), dtype=torch.float64).pin_memory()
+    h2d = sup_h.numel() * 8 + cost_h.numel() * 8
+    d2h = out_xh.numel() * 8 + out_yh.numel() * 8
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e2e_optimal = 0
-    for k in range(args.warmup, args.warmup + args.steps):
-        sup, cost = pinned[k]
-        session.load(objective=cost.numpy(), row_lower=sup.numpy(), row_upper=sup.numpy())
-        e2e_optimal += session.solve()
-        res = session.read(primal=out_x.numpy(), dual=out_y.numpy())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    sup_d = sup_h.to(dev, non_blocking=True)
+    cost_d = cost_h.to(dev, non_blocking=True)
+    res_e2e, _ = solve(sup_d, cost_d, px, py)
+    out_xh.copy_(px, non_blocking=True)
+    out_yh.copy_(py, non_blocking=True)
+    e1.record()
     torch.cuda.synchronize()
-    e2e_elapsed = time.perf_counter() - t0
-    t = torch.tensor([e2e_elapsed], device=dev)
+    t = torch.tensor([e0.elapsed_time(e1) / 1e3], device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.batch * args.steps / float(t.item())
+    e2e_value = world * K * B / float(t.item())
 
-    # Dominant kernel, timed live with CUDA events on the library's stream.
-    tk = session.time_kernels(20)
-    kernel = "k_primal" if tk["primal_ms"] >= tk["dual_ms"] else "k_dual"
-    ms = tk["primal_ms"] if kernel == "k_primal" else tk["dual_ms"]
-    nbytes = tk["primal_bytes"] if kernel == "k_primal" else tk["dual_bytes"]
+    # Roofline of the dominant trial kernel, live durations from the events
+    # captured in the timed loop.
+    s_bytes = 4 if args.precision == "mixed" else 8
+    pb, db = trial_bytes(n, m, nnz, args.slots, s_bytes)
+    kernel = "k_il_primal" if loop["primal_ms"] >= loop["dual_ms"] else "k_il_dual"
+    ms = loop["primal_ms"] if kernel == "k_il_primal" else loop["dual_ms"]
+    nbytes = pb if kernel == "k_il_primal" else db
+    other = "k_il_dual" if kernel == "k_il_primal" else "k_il_primal"
+    oms = loop["dual_ms"] if kernel == "k_il_primal" else loop["primal_ms"]
+    obytes = db if kernel == "k_il_primal" else pb
     peak, peak_kind = peaks()
     achieved = nbytes / (ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": kernel, "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": ncu_traffic(kernel), "algorithmic_bytes_per_launch": nbytes,
-                "launch_ms": round(ms, 5),
-                "other_kernel": {"name": "k_dual" if kernel == "k_primal" else "k_primal",
-                                 "launch_ms": round(tk["dual_ms"] if kernel == "k_primal" else tk["primal_ms"], 5),
-                                 "gbs": round((tk["dual_bytes"] / tk["dual_ms"] if kernel == "k_primal"
-                                               else tk["primal_bytes"] / tk["primal_ms"]) / 1e6, 1)}}
+                "launch_ms": round(ms, 5), "launch_samples": loop["samples"],
+                "other_kernel": {"name": other, "launch_ms": round(oms, 5),
+                                 "gbs": round(obytes / (oms * 1e-3) / 1e9, 1)},
+                "chunk_ms": round(loop["chunk_ms"], 3), "check_stage_ms": round(loop["check_ms"], 3)}
 
     line = {"metric": METRIC, "value": round(value, 2), "unit": "LPs/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(1e3 * elapsed_max / args.steps, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 iterations, f64 checks"
-            if args.precision == "mixed" else "f64", "data": "synthetic (seeded generators)",
-            "config": config, "optimal_fraction": optimal / (args.batch * args.steps),
+            "steps": K, "warmup": W, "ms_per_step": round(1e3 * elapsed_max / K, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "mixed" else "f64",
+            "data": "synthetic (seeded generators); random-init network trained in the run",
+            "config": config, "optimal_fraction": optimal / (K * B),
+            "mean_iterations": float(iters.mean()), "max_iterations": int(iters.max()),
+            "max_relative_kkt": float(np.max(np.maximum(np.maximum(res["primal_residual"], res["dual_residual"]),
+                                                         res["relative_gap"]))),
             "clocks": clocks.summary(), "gpu_launches": int(launches),
-            "e2e": {"value": round(e2e_value, 2), "unit": "LPs/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "optimal_fraction": e2e_optimal / (args.batch * args.steps)},
+            "e2e": {"value": round(e2e_value, 2), "unit": "LPs/s", "h2d_bytes_per_step": h2d // K,
+                    "d2h_bytes_per_step": d2h // K, "optimal_fraction": res_e2e["optimal"] / (K * B)},
             "roofline": roofline}
+    if train_info is not None:
+        line["training"] = train_info
 
     if rank == 0 and not args.no_extras:
-        line["plain_gpu_fp64_single"] = plain_gpu(graph, steps_in[-1], args.tol)
-        line["speedup_vs_plain_gpu_fp64"] = round(value / world / line["plain_gpu_fp64_single"]["lps_per_s"], 2)
+        line["extras"] = extras(args, session, graph, sup_all[timed], cost_all[timed], steps_in[-1],
+                                value, iters, solve)
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args, graph, steps_in[-1])
+        line["cpu_baseline"] = cpu_baseline(args, graph, steps_in[-1], res)
     session.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+
+
+def extras(args, session, graph, sup, cost, inputs, value, iters, solve):
+    """Side measurements: the same instances cold (the learned gain), plain
+    FP64 one-LP-per-call GPU PDLP (the comparison the target is quoted
+    against), and the trial kernels on the single large LP."""
+    import torch
+    out = {}
+    if not args.cold:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cold, _ = solve(sup, cost, warm=False)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out["cold_batched"] = {"lps_per_s": round(sup.shape[0] / dt, 2),
+                               "mean_iterations": float(cold["iterations"].mean()),
+                               "max_iterations": int(cold["iterations"].max()),
+                               "optimal_fraction": cold["optimal"] / sup.shape[0]}
+        out["learned_gain"] = {"lps_ratio": round(value / out["cold_batched"]["lps_per_s"], 3),
+                               "iteration_ratio": round(float(iters.mean()) / float(cold["iterations"].mean()), 3)}
+    out["plain_gpu_fp64_single"] = plain_gpu(graph, inputs, args.tol)
+    out["speedup_vs_plain_gpu_fp64"] = round(value / out["plain_gpu_fp64_single"]["lps_per_s"], 2)
+    out["large_lp_trial_kernels"] = large_lp_kernels()
+    return out
 
 
 def plain_gpu(graph, inputs, tol, count=6):
@@ -308,18 +399,44 @@ def plain_gpu(graph, inputs, tol, count=6):
     return {"lps_per_s": round(count / dt, 3), "instances": count, "mean_iterations": float(np.mean(iters))}
 
 
-def cpu_baseline(args, graph, inputs):
+def large_lp_kernels():
+    """PDHG trial kernels (fused SpMV + projections) on the single large LP
+    (500,000 x 1,000,000, 8.2M nonzeros), FP64 and FP32, timed with CUDA
+    events: GB/s of algorithmic bytes."""
+    from optimisation_solver_b200 import generators as g
+    from optimisation_solver_b200.lp import PdlpOptions
+    from optimisation_solver_b200.session import Session
+    p = g.large_lp(0)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        S = Session(p.lp, 1, PdlpOptions(), precision=prec)
+        S.load()
+        tk = S.time_kernels(10)
+        S.close()
+        out[prec] = {"primal_us": round(tk["primal_ms"] * 1e3, 1), "dual_us": round(tk["dual_ms"] * 1e3, 1),
+                     "primal_gbs": round(tk["primal_bytes"] / tk["primal_ms"] / 1e6, 1),
+                     "dual_gbs": round(tk["dual_bytes"] / tk["dual_ms"] / 1e6, 1)}
+    return out
+
+
+def cpu_baseline(args, graph, inputs, res):
+    """The reference's CPU PDLP (built from its sources) on a bounded sample of
+    the same instances, with every host thread; also the objective error of
+    the device results for those instances against it."""
     from oracle.oracle import available
     kind = "ref_fast" if available("ref_fast") else "port"
     threads = os.cpu_count() or 1
     supply, cost = inputs
     k = min(args.cpu_sample, supply.shape[0])
-    seconds, statuses = cpu_solve_sample(kind, graph, supply[:k], cost[:k], args.tol, threads)
+    seconds, statuses, objs = cpu_solve_sample(kind, graph, supply[:k], cost[:k], args.tol, threads)
+    last = res["primal_objective"][-args.batch:][:k]
+    rel = np.abs(last - np.array(objs)) / (1.0 + np.abs(np.array(objs)))
     return {"value": round(k / seconds, 3), "unit": "LPs/s", "cores": threads,
             "kind": "reference" if kind == "ref_fast" else "port",
-            "sample": f"{k} instances of the same family and tolerance, instance-parallel, "
-                      f"one solver thread each, {seconds:.1f} s",
-            "optimal_fraction": statuses.count("optimal") / k}
+            "sample": f"{k} instances of the last step, instance-parallel, one solver thread each, "
+                      f"{seconds:.1f} s",
+            "optimal_fraction": statuses.count("optimal") / k,
+            "device_vs_cpu_objective_rel_max": float(rel.max())}
 
 
 def reference_arm(args, world, rank, graph, config):
@@ -339,7 +456,7 @@ def reference_arm(args, world, rank, graph, config):
     total = 0.0
     optimal = 0
     for k in range(args.warmup, args.warmup + args.steps):
-        seconds, statuses = cpu_solve_sample(kind, graph, inputs[k][0], inputs[k][1], args.tol, threads)
+        seconds, statuses, _ = cpu_solve_sample(kind, graph, inputs[k][0], inputs[k][1], args.tol, threads)
         total += seconds
         optimal += statuses.count("optimal")
     value = per_step * args.steps / total
@@ -347,8 +464,8 @@ def reference_arm(args, world, rank, graph, config):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generators)",
-            "config": dict(config, batch=per_step), "impl": "reference",
-            "optimal_fraction": optimal / (per_step * args.steps),
+            "config": dict(config, batch=per_step, warm_start="cold (the reference has no warm start)"),
+            "impl": "reference", "optimal_fraction": optimal / (per_step * args.steps),
             "cpu_baseline": {"value": round(value, 3), "unit": "LPs/s", "cores": threads,
                              "kind": "reference" if kind == "ref_fast" else "port",
                              "sample": f"{per_step} instances per step, instance-parallel"},

@@ -106,6 +106,13 @@ enum {
     PDLPGPU_PRECISION_MIXED = 1   /* FP32 A and iterates; FP64 checks, objective, final FP64 stage */
 };
 
+/* Device layout of a session's trial kernels. */
+enum {
+    PDLPGPU_LAYOUT_AUTO = 0,         /* interleaved for sessions of 16 or more instances */
+    PDLPGPU_LAYOUT_SELL = 1,         /* one SELL-G matrix walk per instance */
+    PDLPGPU_LAYOUT_INTERLEAVED = 2   /* vectors [line][instance]; a warp serves 32 instances */
+};
+
 /* Extensions with no counterpart in PdlpOptions. Zero means "default". */
 typedef struct pdlpgpu_ext_options {
     int32_t precision;             /* PDLPGPU_PRECISION_* */
@@ -117,7 +124,9 @@ typedef struct pdlpgpu_ext_options {
     int32_t fp32_switch_factor;    /* mixed: FP64 stage once KKT <= factor * tol fails to improve (0 = 1) */
     int32_t disable_graphs;        /* 1: launch kernels directly instead of CUDA graphs */
     int32_t cta_slots;             /* SpMV tuning: matrix slots per CTA (0 = autotune) */
-    int32_t reserved[7];
+    int32_t layout;                /* sessions: PDLPGPU_LAYOUT_* */
+    int32_t lane_instances;        /* interleaved layout: instances per lane, 1, 2 or 4 (0 = auto) */
+    int32_t reserved[5];
 } pdlpgpu_ext_options;
 
 /* Optional warm start (this engine's extension; the reference starts from the

@@ -78,6 +78,14 @@ int32_t pdlpgpu_session_stream(pdlpgpu_session* session, int32_t on_device, int6
 int32_t pdlpgpu_session_last_timing(pdlpgpu_session* session, double* device_seconds,
                                     int64_t* launches);
 
+/* Live timing of the last solve or stream: CUDA events recorded inside the
+ * captured iteration loop around the two kernels of four trial slots of every
+ * chunk (its first, second, middle and last slot). out[15] = {primal ms per
+ * launch, dual ms per launch, samples, ms per chunk, chunks, device seconds of
+ * the loop, ms per chunk in the check stage, then primal and dual ms per
+ * launch at each of the four slots}. */
+int32_t pdlpgpu_session_loop_timing(pdlpgpu_session* session, double* out);
+
 /* Times the two PDHG trial kernels with CUDA events on the session's stream,
  * `reps` launches each, with every instance forced active and no state
  * change. out[6] = {primal ms per launch, dual ms per launch, primal

@@ -506,6 +506,12 @@ int32_t pdlpgpu_session_last_timing(pdlpgpu_session* s, double* device_seconds, 
     return 0;
 }
 
+int32_t pdlpgpu_session_loop_timing(pdlpgpu_session* s, double* out) {
+    if (s == nullptr || out == nullptr) return -1;
+    s->engine.loop_timing(out);
+    return 0;
+}
+
 int32_t pdlpgpu_session_time_kernels(pdlpgpu_session* s, int32_t reps, double* out) {
     if (s == nullptr || reps <= 0) return -1;
     try {

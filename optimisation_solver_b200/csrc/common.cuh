@@ -88,7 +88,8 @@ struct InstanceCtl {
     int32_t have_avg_at_check;
     int32_t fp64_stage;     // mixed solves: 1 once the FP64 stage has started
     int32_t stall_checks;
-    int32_t pad0, pad1;
+    int32_t ibuf;           // interleaved layout: buffer holding the committed iterate
+    int32_t il_sync;        // interleaved layout: the iterate was copied out for a check
     // --- counters
     int64_t iteration;       // main phase: committed iterations (state.iteration)
     int64_t step_trials;     // main phase trials

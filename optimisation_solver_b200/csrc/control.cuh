@@ -182,7 +182,7 @@ __device__ inline void average_add(InstanceCtl& c, double weight) {   // iterate
 
 // After the two halves of one trial: finiteness test, linesearch decision,
 // commit, averaging and the check boundary.
-__device__ __noinline__ void trial_control(InstanceCtl& c, const DeviceOptions& o, double pmove,
+inline __device__ __noinline__ void trial_control(InstanceCtl& c, const DeviceOptions& o, double pmove,
                                      double dmove, double inter, int32_t n_cols) {
     c.pending_avg = 0;
     c.dbg[0] = pmove;
@@ -241,6 +241,22 @@ __device__ __noinline__ void trial_control(InstanceCtl& c, const DeviceOptions& 
         }
     }
 }
+
+// The instance runs trial kernels of working precision T now.
+template <class T>
+__device__ __forceinline__ bool precision_matches(const InstanceCtl& c) {
+    return (c.fp64_stage != 0) == (sizeof(T) == 8);
+}
+
+template <class T>
+__device__ __forceinline__ bool trial_active(const InstanceCtl& c) {
+    return c.phase != kPhaseDone && c.stage == kStageTrial && precision_matches<T>(c);
+}
+
+// Smallest dual step of the trial (a zero step would stall the prox).
+template <class T> __device__ __forceinline__ T min_dual_step();
+template <> __device__ __forceinline__ double min_dual_step<double>() { return 1e-300; }
+template <> __device__ __forceinline__ float min_dual_step<float>() { return 1e-37f; }
 
 // RestartController::choose (restart_controller.cpp:8-63). Returns 0 none,
 // 1 current, 2 average; candidate score through `score`.

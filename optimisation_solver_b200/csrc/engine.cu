@@ -80,6 +80,8 @@ void fill_value(std::vector<T>& v, size_t n, T x) { v.assign(n, x); }
 Engine::Engine(int device) : device_(device) {}
 
 Engine::~Engine() {
+    for (cudaEvent_t e : tev_)
+        if (e) cudaEventDestroy(e);
     for (void* q : extra_) cudaFree(q);
     if (graph_) cudaGraphExecDestroy(graph_);
     if (arena_) cudaFree(arena_);
@@ -153,6 +155,8 @@ bool Engine::prepare(const SolveSpec& spec) {
     if (!check(cudaGetDeviceProperties(&prop, device_), "cudaGetDeviceProperties")) return false;
     sms_ = prop.multiProcessorCount;
     if (!check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
+    for (cudaEvent_t& e : tev_)
+        if (e == nullptr && !check(cudaEventCreate(&e), "cudaEventCreate")) return false;
 
     // Layouts: one per device instance, or one shared.
     std::vector<HostCsr> csrT;
@@ -654,8 +658,10 @@ void Engine::enqueue_trial(const Work<T>& w) {
     launches_ += 2;
 }
 
-void Engine::enqueue_check_stage() {
+void Engine::enqueue_check_stage(bool il_sync) {
     const int V = tuning_.vector_width;
+    const bool sync = il_sync && il_;
+    if (sync) il_move_iterates(true, kIlAtCheck, nullptr);
     if (mixed_) launch_check_prep<float>(g_, w32_, dopt_, stream_);
     launch_check_prep<double>(g_, w64_, dopt_, stream_);
     launch_check_spmv(g_, dopt_, V, stream_);
@@ -663,19 +669,110 @@ void Engine::enqueue_check_stage() {
     launch_check_apply<double>(g_, w64_, dopt_, stream_);
     if (mixed_) launch_refresh<float>(g_, w32_, dopt_, V, stream_);
     launch_refresh<double>(g_, w64_, dopt_, V, stream_);
+    if (sync) il_move_iterates(false, kIlSynced, nullptr);
     cudaMemsetAsync(d_active_, 0, sizeof(int32_t), stream_);
     launch_finalize(g_, count_, d_active_, stream_);
-    launches_ += mixed_ ? 8 : 5;
+    launches_ += check_stage_launches(il_sync);
+}
+
+void Engine::record_timing(int k) {
+    // Event nodes in the captured graph (plain records when not capturing).
+    cudaEventRecordWithFlags(tev_[k], stream_, cudaEventRecordExternal);
+}
+
+int Engine::timed_position(int k, int slots) const {
+    // First, second, middle and last slot of the chunk (distinct slots only).
+    const int pos[kTimedSlots] = {0, 1, slots / 2, slots - 1};
+    for (int p = 0; p < kTimedSlots; ++p) {
+        bool dup = false;
+        for (int q = 0; q < p; ++q) dup = dup || pos[q] == pos[p];
+        if (!dup && pos[p] == k) return p;
+    }
+    return -1;
 }
 
 void Engine::enqueue_chunk(int slots) {
     // A mixed solve iterates in FP32; the FP64 trial kernels are captured only
-    // for the FP64 stage graph.
+    // for the FP64 stage graph. Four slots' kernels are bracketed by timing
+    // events.
+    record_timing(0);
     for (int k = 0; k < slots; ++k) {
-        if (mixed_ && !fp64_graph_) enqueue_trial<float>(w32_);
-        else enqueue_trial<double>(w64_);
+        const int p = timed_position(k, slots);
+        if (p >= 0) record_timing(3 + 3 * p);
+        if (il_) {
+            if (mixed_) launch_il_primal<float>(il32_, g_.ctl, 0, k, stream_);
+            else launch_il_primal<double>(il64_, g_.ctl, 0, k, stream_);
+            if (p >= 0) record_timing(4 + 3 * p);
+            if (mixed_) launch_il_dual<float>(il32_, g_.ctl, dopt_, 0, k, stream_);
+            else launch_il_dual<double>(il64_, g_.ctl, dopt_, 0, k, stream_);
+        } else if (mixed_ && !fp64_graph_) {
+            launch_primal<float>(g_, w32_, dopt_, tuning_.vector_width, stream_);
+            if (p >= 0) record_timing(4 + 3 * p);
+            launch_dual<float>(g_, w32_, dopt_, tuning_.vector_width, stream_);
+        } else {
+            launch_primal<double>(g_, w64_, dopt_, tuning_.vector_width, stream_);
+            if (p >= 0) record_timing(4 + 3 * p);
+            launch_dual<double>(g_, w64_, dopt_, tuning_.vector_width, stream_);
+        }
+        launches_ += 2;
+        if (p >= 0) record_timing(5 + 3 * p);
     }
-    enqueue_check_stage();
+    record_timing(1);
+    enqueue_check_stage(true);
+    record_timing(2);
+}
+
+void Engine::timing_reset() {
+    for (int p = 0; p < kTimedSlots; ++p) t_primal_[p] = t_dual_[p] = 0.0;
+    t_chunk_ = t_check_ = 0.0;
+    t_samples_ = t_chunks_ = 0;
+}
+
+void Engine::timing_collect(int slots) {
+    float c = 0.f, d = 0.f;
+    if (cudaEventElapsedTime(&c, tev_[0], tev_[2]) != cudaSuccess ||
+        cudaEventElapsedTime(&d, tev_[1], tev_[2]) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    t_chunk_ += c;
+    t_check_ += d;
+    ++t_chunks_;
+    bool all = true;
+    float a[kTimedSlots] = {}, b[kTimedSlots] = {};
+    for (int k = 0; k < slots; ++k) {
+        const int p = timed_position(k, slots);
+        if (p < 0) continue;
+        all = all && cudaEventElapsedTime(&a[p], tev_[3 + 3 * p], tev_[4 + 3 * p]) == cudaSuccess &&
+              cudaEventElapsedTime(&b[p], tev_[4 + 3 * p], tev_[5 + 3 * p]) == cudaSuccess;
+    }
+    cudaGetLastError();
+    if (!all || slots < kTimedSlots) return;
+    for (int p = 0; p < kTimedSlots; ++p) {
+        t_primal_[p] += a[p];
+        t_dual_[p] += b[p];
+    }
+    ++t_samples_;
+}
+
+void Engine::loop_timing(double* out) const {
+    double p = 0.0, d = 0.0;
+    for (int k = 0; k < kTimedSlots; ++k) {
+        p += t_primal_[k];
+        d += t_dual_[k];
+    }
+    const double n = static_cast<double>(t_samples_) * kTimedSlots;
+    out[0] = t_samples_ ? p / n : 0.0;
+    out[1] = t_samples_ ? d / n : 0.0;
+    out[2] = static_cast<double>(t_samples_ * kTimedSlots);
+    out[3] = t_chunks_ ? t_chunk_ / t_chunks_ : 0.0;
+    out[4] = static_cast<double>(t_chunks_);
+    out[5] = device_seconds_;
+    out[6] = t_chunks_ ? t_check_ / t_chunks_ : 0.0;
+    for (int k = 0; k < kTimedSlots; ++k) {
+        out[7 + 2 * k] = t_samples_ ? t_primal_[k] / t_samples_ : 0.0;
+        out[8 + 2 * k] = t_samples_ ? t_dual_[k] / t_samples_ : 0.0;
+    }
 }
 
 bool Engine::build_graph(int slots) {
@@ -689,6 +786,7 @@ bool Engine::build_graph(int slots) {
     const bool ok = check(cudaGraphInstantiate(&graph_, graph, 0), "graph instantiate");
     cudaGraphDestroy(graph);
     graph_slots_ = slots;
+    graph_family_ = il_family_;
     return ok;
 }
 
@@ -699,10 +797,10 @@ bool Engine::run() {
         return false;
     if (!check(cudaStreamSynchronize(stream_), "setup")) return false;
     const int slack = spec_.ext.chunk_slack > 0 ? spec_.ext.chunk_slack : 4;
-    const int slots = std::max(1, std::min(o.termination_check_frequency + slack, 1024));
+    const int slots = chunk_slots();
     const bool graphs = spec_.ext.disable_graphs == 0;
     if (*h_active_ != 0 && graphs && graph_ == nullptr && !build_graph(slots)) return false;
-    const int per_chunk = 2 * slots + (mixed_ ? 8 : 5);
+    const int per_chunk = 2 * slots + check_stage_launches(true);
     const int64_t trials_bound =
         (std::max<int64_t>(o.iteration_limit, 0) + std::max(o.polishing_iterations, 0) + 2) *
         std::max(o.maximum_step_trials, 1);
@@ -711,6 +809,7 @@ bool Engine::run() {
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, stream_);
+    timing_reset();
     int64_t chunks = 0;
     while (*h_active_ != 0) {
         if (chunks >= max_chunks) {
@@ -726,6 +825,7 @@ bool Engine::run() {
         ++chunks;
         cudaMemcpyAsync(h_active_, d_active_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
         if (!check(cudaStreamSynchronize(stream_), "iteration loop")) break;
+        timing_collect(slots);
     }
     cudaEventRecord(e1, stream_);
     cudaEventSynchronize(e1);
@@ -1093,6 +1193,8 @@ bool Engine::session_create(const pdlpgpu_lp& family, int32_t batch, const pdlpg
             return false;
         session_eta_max_ = c0.eta_max;
     }
+    il_ = ext.layout == PDLPGPU_LAYOUT_INTERLEAVED || (ext.layout == PDLPGPU_LAYOUT_AUTO && batch >= 16);
+    if (il_ && !(mixed_ ? il_build(il32_, w32_) : il_build(il64_, w64_))) return false;
     return check(cudaStreamSynchronize(stream_), "session setup");
 }
 
@@ -1122,6 +1224,10 @@ bool Engine::session_load(bool on_device, const double* c, const double* rl, con
               load(ru, const_cast<double*>(g_.ru_orig), fam_[2], false) &&
               load(xl, const_cast<double*>(g_.xl_orig), fam_[3], true) &&
               load(xu, const_cast<double*>(g_.xu_orig), fam_[4], true);
+    if (il_)
+        il_set_family((c == nullptr ? 1 << kIlC : 0) | (rl == nullptr ? 1 << kIlRl : 0) |
+                      (ru == nullptr ? 1 << kIlRu : 0) | (xl == nullptr ? 1 << kIlXl : 0) |
+                      (xu == nullptr ? 1 << kIlXu : 0));
     g_.warm_x = nullptr;
     g_.warm_y = nullptr;
     if (wx != nullptr) ok = ok && load(wx, warm_x_, nullptr, true), g_.warm_x = warm_x_;
@@ -1152,9 +1258,14 @@ bool Engine::session_solve(int32_t* optimal) {
     launch_refresh<double>(g_, w64_, dopt_, tuning_.vector_width, stream_);
     const int64_t before = launches_;
     enqueue_check_stage();
+    if (il_) {
+        il_move_statics(kIlAll, nullptr);
+        il_move_iterates(false, kIlAll, nullptr);
+    }
     launches_ = before;
     if (!check(cudaGetLastError(), "session start")) return false;
     launches_ = 0;
+    if (!ensure_graph()) return false;
     if (!run()) return false;
     std::vector<InstanceCtl> ctl(static_cast<size_t>(count_));
     if (!check(cudaMemcpyAsync(ctl.data(), g_.ctl, ctl.size() * sizeof(InstanceCtl), cudaMemcpyDeviceToHost, stream_), "download") ||
@@ -1209,8 +1320,21 @@ bool Engine::time_kernels(int reps, double* out) {
     cudaEvent_t e[4];
     for (auto& ev : e) cudaEventCreate(&ev);
     const int V = tuning_.vector_width;
-    auto primal = [&] { if (mixed_) launch_primal<float>(gm, w32_, dopt_, V, stream_); else launch_primal<double>(gm, w64_, dopt_, V, stream_); };
-    auto dual = [&] { if (mixed_) launch_dual<float>(gm, w32_, dopt_, V, stream_); else launch_dual<double>(gm, w64_, dopt_, V, stream_); };
+    // The interleaved kernels in timing mode write their trial buffers for
+    // every lane, which may hold committed points: the iterates are undefined
+    // afterwards (every solve starts from a fresh setup).
+    auto primal = [&] {
+        if (il_ && mixed_) launch_il_primal<float>(il32_, g_.ctl, 1, 0, stream_);
+        else if (il_) launch_il_primal<double>(il64_, g_.ctl, 1, 0, stream_);
+        else if (mixed_) launch_primal<float>(gm, w32_, dopt_, V, stream_);
+        else launch_primal<double>(gm, w64_, dopt_, V, stream_);
+    };
+    auto dual = [&] {
+        if (il_ && mixed_) launch_il_dual<float>(il32_, g_.ctl, dopt_, 1, 0, stream_);
+        else if (il_) launch_il_dual<double>(il64_, g_.ctl, dopt_, 1, 0, stream_);
+        else if (mixed_) launch_dual<float>(gm, w32_, dopt_, V, stream_);
+        else launch_dual<double>(gm, w64_, dopt_, V, stream_);
+    };
     primal();
     dual();
     cudaEventRecord(e[0], stream_);
@@ -1234,6 +1358,23 @@ bool Engine::time_kernels(int reps, double* out) {
     const double N = static_cast<double>(cols_total_), R = static_cast<double>(rows_total_);
     out[0] = mp / reps;
     out[1] = md / reps;
+    if (il_) {
+        // Per instance: the line's own vectors (x read, x' written, and each
+        // problem vector loaded per instance) and the gathered vector once;
+        // once for the batch: the matrix (value, index, row pointer) and the
+        // broadcast vectors (preconditioner and family vectors).
+        auto own = [&](int k) { return ((il_family_ >> k) & 1) ? 0.0 : 1.0; };
+        const double B = count_, n = info_[0].n, m = info_[0].m, nnz = e_at;
+        const double col_own = 2.0 + own(kIlC) + own(kIlXl) + own(kIlXu);
+        const double col_fam = 2.0 + (3.0 - own(kIlC) - own(kIlXl) - own(kIlXu));
+        const double row_own = 4.0 + own(kIlRl) + own(kIlRu);
+        const double row_fam = 2.0 + (2.0 - own(kIlRl) - own(kIlRu));
+        out[2] = B * n * col_own * T + n * col_fam * T + nnz * (T + 4.0) + (n + 1) * 8.0 + B * m * T;
+        out[3] = B * m * row_own * T + m * row_fam * T + nnz * (T + 4.0) + (m + 1) * 8.0 + B * n * T;
+        out[4] = 0.0;
+        out[5] = 0.0;
+        return true;
+    }
     out[2] = e_at * (T + 4.0) + N * 7.0 * T + R * T;
     out[3] = e_a * (T + 4.0) + R * 8.0 * T + N * T;
     out[4] = s_at - e_at;
@@ -1246,10 +1387,14 @@ bool Engine::time_kernels(int reps, double* out) {
 // Streams
 // ---------------------------------------------------------------------------
 bool Engine::ensure_graph() {
+    if (graph_ != nullptr && il_ && graph_family_ != il_family_) {
+        // The captured interleaved kernels address the family vectors of the
+        // load they were captured with.
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
     if (graph_ != nullptr || spec_.ext.disable_graphs) return true;
-    const int slack = spec_.ext.chunk_slack > 0 ? spec_.ext.chunk_slack : 4;
-    const int slots = std::max(1, std::min(spec_.opt.termination_check_frequency + slack, 1024));
-    return build_graph(slots);
+    return build_graph(chunk_slots());
 }
 
 bool Engine::session_stream(bool on_device, int64_t N, const double* const in[5], const double* wx,
@@ -1301,6 +1446,11 @@ bool Engine::session_stream(bool on_device, int64_t N, const double* const in[5]
         if (out_y && !dalloc(doy, static_cast<size_t>(N * m), temp)) return false;
     }
     const bool warm = wx != nullptr || wy != nullptr;
+    if (il_) {
+        int32_t family = 0;
+        for (int k = 0; k < kIlVecs; ++k) family |= in[k] == nullptr ? 1 << k : 0;
+        il_set_family(family);
+    }
     if (!ensure_graph()) return false;
 
     launch_retire(g_, B, stream_);
@@ -1309,8 +1459,8 @@ bool Engine::session_stream(bool on_device, int64_t N, const double* const in[5]
     std::vector<InstanceCtl> ctl(static_cast<size_t>(B));
     int64_t next = 0;
     const int slack = spec_.ext.chunk_slack > 0 ? spec_.ext.chunk_slack : 4;
-    const int slots = graph_slots_ > 0 ? graph_slots_ : std::max(1, std::min(o.termination_check_frequency + slack, 1024));
-    const int per_chunk = 2 * slots + (mixed_ ? 8 : 5);
+    const int slots = graph_slots_ > 0 ? graph_slots_ : chunk_slots();
+    const int per_chunk = 2 * slots + check_stage_launches(true);
     launches_ = 0;
 
     auto upload_slots = [&]() {
@@ -1363,6 +1513,11 @@ bool Engine::session_stream(bool on_device, int64_t N, const double* const in[5]
         launch_refresh<double>(g_, w64_, dopt_, tuning_.vector_width, stream_);
         enqueue_check_stage();
         launches_ += 12;
+        if (il_) {
+            il_move_statics(kIlMasked, d_mask_);
+            il_move_iterates(false, kIlMasked, d_mask_);
+            launches_ += 2;
+        }
         return check(cudaGetLastError(), "refill");
     };
     auto harvest = [&]() {
@@ -1399,6 +1554,7 @@ bool Engine::session_stream(bool on_device, int64_t N, const double* const in[5]
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, stream_);
+    timing_reset();
     bool ok = refill();
     const int64_t trials_bound =
         (std::max<int64_t>(o.iteration_limit, 0) + std::max(o.polishing_iterations, 0) + 2) *
@@ -1410,6 +1566,7 @@ bool Engine::session_stream(bool on_device, int64_t N, const double* const in[5]
         ok = check(cudaMemcpyAsync(done.data(), d_done_, done.size() * 4, cudaMemcpyDeviceToHost, stream_), "poll") &&
              check(cudaStreamSynchronize(stream_), "poll");
         if (!ok) break;
+        if (chunks > 0) timing_collect(slots);
         ok = harvest() && refill();
         if (!ok) break;
         bool active = false;

@@ -1,6 +1,7 @@
 // engine.hpp -- host side of the device PDLP engine.
 #pragma once
 
+#include "interleaved.cuh"
 #include "kernels.cuh"
 #include "layout.hpp"
 #include "pdlpgpu.h"
@@ -63,6 +64,13 @@ public:
                         const double* wy, const double* ww, double* out_x, double* out_y,
                         int32_t* status, int64_t* iterations, double* stats);
     int32_t count() const { return count_; }
+    // Live durations over the last solve or stream, from CUDA events captured
+    // in the iteration graph around the two kernels of four trial slots of
+    // every chunk (first, second, middle, last): out[15] = {primal ms per
+    // launch, dual ms per launch, samples, chunk ms, chunks, device seconds of
+    // the loop, check-stage ms per chunk, then primal and dual ms at each of
+    // the four positions}.
+    void loop_timing(double* out) const;
 
     // --- component tests (single instance, internal order handled here) ---
     bool component_spmv(int transpose, int values, const double* in, double* out);
@@ -79,7 +87,21 @@ private:
     template <class T> void enqueue_trial(const Work<T>& w);
     template <class T> void enqueue_check(const Work<T>& w);
     void enqueue_chunk(int slots);
-    void enqueue_check_stage();
+    // The check stage; with `il_sync` the iterates of the instances at a
+    // check are moved out of the interleaved layout first and back after.
+    void enqueue_check_stage(bool il_sync = false);
+    int check_stage_launches(bool il_sync) const;
+    int chunk_slots() const;
+    // --- batch-interleaved layout (sessions)
+    template <class T> bool il_build(Interleaved<T>& il, const Work<T>& w);
+    void il_set_family(int32_t family);
+    void il_enqueue_trial(int slot, int measure);
+    template <class T> IlMove<T> il_iterates(const Interleaved<T>& il, const Work<T>& w,
+                                             bool to_planar, int select, const int32_t* mask) const;
+    template <class T> IlMove<T> il_statics(const Interleaved<T>& il, const Work<T>& w, int select,
+                                            const int32_t* mask) const;
+    void il_move_iterates(bool to_planar, int select, const int32_t* mask);
+    void il_move_statics(int select, const int32_t* mask);
     bool check(cudaError_t e, const char* what);
     bool build_graph(int slots);
     bool ensure_graph();
@@ -148,6 +170,24 @@ private:
     int32_t* d_done_ = nullptr;       // stream: finished flags
     int32_t* d_zero_perm_ = nullptr;  // {0}: identity permutation of length 1
     pdlpgpu_lp family_{};
+    // batch-interleaved layout of the trial kernels (sessions)
+    bool il_ = false;
+    Interleaved<float> il32_{};
+    Interleaved<double> il64_{};
+    int32_t il_family_ = (1 << kIlVecs) - 1;   // vectors every instance takes from the family
+    int32_t graph_family_ = -1;                // il_family_ captured in graph_
+    // live timing events of the chunk: [0] start, [1] end of the trial slots,
+    // [2] end; then for each sampled slot position p (first, second, middle,
+    // last): [3 + 3p] trial start, [4 + 3p] between the halves, [5 + 3p] end
+    static constexpr int kTimedSlots = 4;
+    cudaEvent_t tev_[3 + 3 * kTimedSlots] = {};
+    double t_primal_[kTimedSlots] = {}, t_dual_[kTimedSlots] = {};
+    double t_chunk_ = 0.0, t_check_ = 0.0;
+    int64_t t_samples_ = 0, t_chunks_ = 0;
+    void timing_reset();
+    void timing_collect(int slots);
+    void record_timing(int k);
+    int timed_position(int k, int slots) const;
 };
 
 const char* message_text(int32_t id);

@@ -1,0 +1,892 @@
+// interleaved.cu -- PDHG trial kernels over the batch-interleaved layout of a
+// shared-matrix session, and the transposes between it and the per-instance
+// layout the checks use.
+//
+// Per trial (pdlp_engine/src/pdhg_kernel.cpp:47-187), lane b of a warp is
+// instance group * 32 + b and the warp walks one line:
+//   k_il_primal  column j: g = c + A'y, x' = clip(x - (eta/omega) tau g),
+//                sum dx^2/tau; the owed iterate-average update of x
+//                (iterate_average.cpp:40-82)
+//   k_il_dual    row i: A x', extrapolation 2Ax' - Ax, dual prox, sum
+//                dy^2/sigma and dy'(A dx); the owed average update of y; then,
+//                in the last CTA of each group, the linesearch decision and
+//                commit of its 32 instances (trial_control, one lane each).
+// Sums are per lane: each CTA adds its warps' values in warp order and
+// writes one partial per lane; the deciding CTA adds the partials in CTA
+// order, so a run is bitwise reproducible and needs no atomics on data.
+#include "control.cuh"
+#include "interleaved.cuh"
+
+namespace pdlpgpu {
+namespace {
+
+constexpr int kIlWarps = 8;
+constexpr int kIlThreads = kIlWarps * 32;
+
+// True in every thread of the CTA that arrives last of `expected` CTAs
+// (and resets the counter). Everything written before is visible to it.
+__device__ __forceinline__ bool arrive_last_cta(int32_t* counter, int expected) {
+    __shared__ int last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int prev = atomicAdd(counter, 1);
+        last = prev == expected - 1;
+        if (last) *counter = 0;
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last != 0;
+}
+
+// V consecutive elements (one 4/8/16-byte access).
+template <class T, int V>
+struct Pack;
+template <> struct Pack<float, 1> { using type = float; };
+template <> struct Pack<float, 2> { using type = float2; };
+template <> struct Pack<float, 4> { using type = float4; };
+template <> struct Pack<double, 1> { using type = double; };
+template <> struct Pack<double, 2> { using type = double2; };
+
+template <class T, int V>
+__device__ __forceinline__ void ldv(const T* p, T (&o)[V]) {
+    if constexpr (V == 1) {
+        o[0] = *p;
+    } else if constexpr (V == 2) {
+        const auto v = *reinterpret_cast<const typename Pack<T, 2>::type*>(p);
+        o[0] = v.x; o[1] = v.y;
+    } else {
+        const auto v = *reinterpret_cast<const typename Pack<T, 4>::type*>(p);
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    }
+}
+
+template <class T, int V>
+__device__ __forceinline__ void stv(T* p, const T (&o)[V]) {
+    if constexpr (V == 1) {
+        *p = o[0];
+    } else if constexpr (V == 2) {
+        typename Pack<T, 2>::type v;
+        v.x = o[0]; v.y = o[1];
+        *reinterpret_cast<typename Pack<T, 2>::type*>(p) = v;
+    } else {
+        typename Pack<T, 4>::type v;
+        v.x = o[0]; v.y = o[1]; v.z = o[2]; v.w = o[3];
+        *reinterpret_cast<typename Pack<T, 4>::type*>(p) = v;
+    }
+}
+
+// Stores the active elements only (all of them with one access when every
+// instance of the lane is active): an idle instance's buffer may hold its
+// committed point.
+template <class T, int V>
+__device__ __forceinline__ void stv_masked(T* p, const T (&o)[V], uint32_t mask) {
+    if (mask == (1u << V) - 1) {
+        stv<T, V>(p, o);
+    } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+            if ((mask >> v) & 1) p[v] = o[v];
+    }
+}
+
+// The V instances of a lane: instance group * G + lane * V + v.
+template <class T, int V>
+struct Lanes {
+    uint32_t active;    // bit v: the instance runs this trial
+    uint32_t pending;   // average update owed
+    uint32_t fix;       // committed point in buffer W (it idled or was rejected)
+    T frac[V];
+    T step[V];          // eta / omega (primal) or eta * omega (dual)
+};
+
+template <class T, int V>
+__device__ __forceinline__ Lanes<T, V> lane_state(const Interleaved<T>& il, const InstanceCtl* ctl,
+                                                  int first, int measure, int R, bool primal) {
+    Lanes<T, V> s{0u, 0u, 0u, {}, {}};
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        s.frac[v] = T(0);
+        s.step[v] = T(0);
+        const int b = first + v;
+        if (b >= il.count) continue;
+        const InstanceCtl& c = ctl[b];
+        const bool act = measure ? true : trial_active<T>(c);
+        if (!act) continue;
+        s.active |= 1u << v;
+        s.step[v] = static_cast<T>(primal ? c.trial_eta / c.trial_omega : c.trial_eta * c.trial_omega);
+        if (measure) continue;
+        if (c.pending_avg) s.pending |= 1u << v;
+        s.frac[v] = static_cast<T>(c.avg_frac);
+        if (c.ibuf != R) s.fix |= 1u << v;
+    }
+    return s;
+}
+
+// Committed values of the lane's V instances at offset e: buffer R, or W for
+// the instances whose point is there.
+template <class T, int V>
+__device__ __forceinline__ void load_committed(const T* R, const T* W, int64_t e, uint32_t fix,
+                                               T (&o)[V]) {
+    ldv<T, V>(R + e, o);
+    if (fix) {
+        T alt[V];
+        ldv<T, V>(W + e, alt);
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+            if ((fix >> v) & 1) o[v] = alt[v];
+    }
+}
+
+// Problem vector k at line `line` for the lane: family vectors are [line].
+template <class T, int V>
+__device__ __forceinline__ void load_vec(const Interleaved<T>& il, int k, bool fam, int64_t line,
+                                         int64_t e, T (&o)[V]) {
+    if (fam) {
+        const T x = __ldg(il.vec[k] + line);
+#pragma unroll
+        for (int v = 0; v < V; ++v) o[v] = x;
+    } else {
+        ldv<T, V>(il.vec[k] + e, o);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per-group sums
+// ---------------------------------------------------------------------------
+// CTA partial of NQ per-instance sums: thread (warp w, lane l) holds the sums
+// of instances l * V + v; warps are added in order. Valid in threads t < G
+// (instance t of the group).
+template <int NQ, int V>
+__device__ __forceinline__ void cta_sums(const double (&acc)[NQ][V], double (&out)[NQ]) {
+    constexpr int G = 32 * V;
+    __shared__ double red[NQ][kIlWarps][G];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+        for (int v = 0; v < V; ++v) red[q][warp][lane * V + v] = acc[q][v];
+    __syncthreads();
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        double s = 0.0;
+        if (t < G) {
+#pragma unroll
+            for (int w = 0; w < kIlWarps; ++w) s += red[q][w][t];
+        }
+        out[q] = s;
+    }
+}
+
+// Sum of `n` (at most kIlBatch) rows of a partials array for instance t, in
+// row order; every load is issued before the first add.
+template <int NQ, int G>
+__device__ __forceinline__ void sum_rows(const double* part, int k0, int n, int t, double (&s)[NQ]) {
+    double v[kIlBatch][NQ];
+#pragma unroll
+    for (int k = 0; k < kIlBatch; ++k)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+            v[k][q] = k < n ? part[(static_cast<int64_t>(k0 + k) * NQ + q) * G + t] : 0.0;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) s[q] = 0.0;
+#pragma unroll
+    for (int k = 0; k < kIlBatch; ++k)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+            if (k < n) s[q] += v[k][q];
+}
+
+// First level of a group sum: the CTA writes its partial; the last CTA of
+// its batch of kIlBatch CTAs writes the batch sum. Returns true in the CTA
+// that completed the batch.
+template <int NQ, int G>
+__device__ __forceinline__ bool batch_sums(const double (&cta)[NQ], double* part, double* part2,
+                                           int32_t* cnt, int ctas, int cta_index) {
+    const int t = threadIdx.x;
+    if (t < G) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) part[(static_cast<int64_t>(cta_index) * NQ + q) * G + t] = cta[q];
+    }
+    const int batch = cta_index / kIlBatch;
+    const int b0 = batch * kIlBatch;
+    const int b1 = b0 + kIlBatch < ctas ? b0 + kIlBatch : ctas;
+    if (!arrive_last_cta(cnt + batch, b1 - b0)) return false;
+    if (t < G) {
+        double s[NQ];
+        sum_rows<NQ, G>(part, b0, b1 - b0, t, s);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) part2[(static_cast<int64_t>(batch) * NQ + q) * G + t] = s[q];
+    }
+    return true;
+}
+
+// Sum of the first `n` rows of a batch-sum array for instance t, in order.
+template <int NQ, int G>
+__device__ __forceinline__ void sum_batches(const double* part2, int n, int t, double (&tot)[NQ]) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) tot[q] = 0.0;
+    for (int k0 = 0; k0 < n; k0 += kIlBatch) {
+        double s[NQ];
+        sum_rows<NQ, G>(part2, k0, n - k0 < kIlBatch ? n - k0 : kIlBatch, t, s);
+        // The chunk sums are added in order; each chunk is itself an in-order
+        // sum, so the total is fixed by n alone.
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) tot[q] += s[q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory staging of a tile's matrix entries (double-buffered: the
+// entries of the next tile are copied while the current one is processed)
+// ---------------------------------------------------------------------------
+template <class T>
+struct Stage {
+    int32_t ptr[kIlTileLines + 1];   // entry offsets relative to the tile
+    int32_t idx[kIlTileEntries];
+    T val[kIlTileEntries];
+};
+
+template <int kBytes>
+__device__ __forceinline__ void copy_async(void* dst, const void* src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(kBytes));
+}
+__device__ __forceinline__ void copy_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void copy_async_wait() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+template <class T>
+__device__ __forceinline__ void stage_tile_async(const IlTile& t, const int64_t* __restrict__ ptr,
+                                                 const int32_t* __restrict__ idx,
+                                                 const T* __restrict__ val, Stage<T>& st) {
+    for (int q = threadIdx.x; q < t.entries; q += blockDim.x) {
+        copy_async<4>(st.idx + q, idx + t.e0 + q);
+        copy_async<sizeof(T)>(st.val + q, val + t.e0 + q);
+    }
+    for (int q = threadIdx.x; q <= t.lines; q += blockDim.x)
+        st.ptr[q] = static_cast<int32_t>(__ldg(ptr + t.line0 + q) - t.e0);
+    copy_async_commit();
+}
+
+// sum_k val[k] * src[idx[k] * bp + ...] for the lane's V instances, entries
+// in order; kU gathers in flight. Instances with `fix` gather their committed
+// values from `alt` (rare).
+template <int kU, class T, int V>
+__device__ __forceinline__ void gather_sum(const int32_t* idx, const T* val, int n,
+                                           const T* __restrict__ src, const T* __restrict__ alt,
+                                           uint32_t fix, int64_t bp, T (&sum)[V]) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) sum[v] = T(0);
+    int k = 0;
+    for (; k + kU <= n; k += kU) {
+        int32_t i[kU];
+        T w[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            i[u] = idx[k + u];
+            w[u] = val[k + u];
+        }
+        T g[kU][V];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) load_committed<T, V>(src, alt, i[u] * bp, fix, g[u]);
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+#pragma unroll
+            for (int v = 0; v < V; ++v) sum[v] += w[u] * g[u][v];
+    }
+    for (; k < n; ++k) {
+        T g[V];
+        load_committed<T, V>(src, alt, idx[k] * bp, fix, g);
+        const T w = val[k];
+#pragma unroll
+        for (int v = 0; v < V; ++v) sum[v] += w * g[v];
+    }
+}
+
+// Lines per warp pass: about four lane-vectors of each kind in flight per
+// warp within 128 registers.
+template <class T, int V>
+constexpr int kPrimalU = (sizeof(T) == 4 ? 4 : 2) / V > 0 ? (sizeof(T) == 4 ? 4 : 2) / V : 1;
+template <class T, int V>
+constexpr int kDualU = (sizeof(T) == 4 && V == 1) ? 2 : 1;
+// Gathers in flight per lane in the dual's entry loop.
+template <int V>
+constexpr int kDualGather = V >= 4 ? 4 : 8;
+
+// ---------------------------------------------------------------------------
+// Primal half
+// ---------------------------------------------------------------------------
+template <class T, int V>
+struct PrimalCtx {
+    const Interleaved<T>* il;
+    Lanes<T, V> ls;
+    const T* XR;
+    const T* XW_read;
+    T* xr;
+    T* xw;
+    const T* YR;
+    const T* YW;
+    T* avg;
+    int64_t col0;      // first instance of the lane
+    bool fc, fl, fu;
+};
+
+// Bounds of a line: one value per lane-instance, or one for all (kFam: both
+// bounds are the family's).
+template <class T, int V, bool kFam>
+struct Bounds {
+    static constexpr int N = kFam ? 1 : V;
+    T lo[N], hi[N];
+    __device__ __forceinline__ T l(int v) const { return lo[kFam ? 0 : v]; }
+    __device__ __forceinline__ T h(int v) const { return hi[kFam ? 0 : v]; }
+};
+
+template <class T, int V, bool kFam>
+__device__ __forceinline__ void load_bounds(const Interleaved<T>& il, int klo, int khi, bool flo,
+                                            bool fhi, int64_t line, int64_t e, Bounds<T, V, kFam>& B) {
+    if constexpr (kFam) {
+        B.lo[0] = __ldg(il.vec[klo] + line);
+        B.hi[0] = __ldg(il.vec[khi] + line);
+    } else {
+        load_vec<T, V>(il, klo, flo, line, e, B.lo);
+        load_vec<T, V>(il, khi, fhi, line, e, B.hi);
+    }
+}
+
+template <class T, int V, bool kFam>
+struct PrimalLine {
+    T c[V], prev[V], a[V];
+    Bounds<T, V, kFam> b;
+    T tj, itj;
+};
+
+template <class T, int V, bool kFam>
+__device__ __forceinline__ void primal_load(const PrimalCtx<T, V>& x, int j, PrimalLine<T, V, kFam>& L) {
+    const Interleaved<T>& il = *x.il;
+    const int64_t e = j * static_cast<int64_t>(il.bp) + x.col0;
+    L.tj = __ldg(il.tau + j);
+    L.itj = __ldg(il.itau + j);
+    load_committed<T, V>(x.XR, x.XW_read, e, x.ls.fix, L.prev);
+    load_vec<T, V>(il, kIlC, x.fc, j, e, L.c);
+    load_bounds<T, V, kFam>(il, kIlXl, kIlXu, x.fl, x.fu, j, e, L.b);
+    if (x.ls.pending) ldv<T, V>(x.avg + e, L.a);
+}
+
+template <class T, int V, bool kFam>
+__device__ __forceinline__ void primal_store(const PrimalCtx<T, V>& x, int j, const PrimalLine<T, V, kFam>& L,
+                                             const T (&sum)[V], double (&moved)[V]) {
+    const Interleaved<T>& il = *x.il;
+    const int64_t e = j * static_cast<int64_t>(il.bp) + x.col0;
+    T upd[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const T gradient = L.c[v] + sum[v];
+        upd[v] = smax(L.b.l(v), smin(L.prev[v] - x.ls.step[v] * L.tj * gradient, L.b.h(v)));
+        const double d = static_cast<double>(upd[v] - L.prev[v]);
+        if ((x.ls.active >> v) & 1) moved[v] += d * d * static_cast<double>(L.itj);
+    }
+    stv_masked<T, V>(x.xw + e, upd, x.ls.active);
+    if (x.ls.pending) {
+        T a[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+            a[v] = ((x.ls.pending >> v) & 1) ? L.a[v] + x.ls.frac[v] * (L.prev[v] - L.a[v]) : L.a[v];
+        stv<T, V>(x.avg + e, a);
+    }
+    if (x.ls.fix) {
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+            if ((x.ls.fix >> v) & 1) x.xr[e + v] = L.prev[v];
+    }
+}
+
+// The lines of one tile: each warp takes lines l, l + 8, ... kU at a time,
+// issuing every line's loads and gathers before its arithmetic.
+template <int kU, bool kStaged, bool kFam, class T, int V>
+__device__ __forceinline__ void primal_tile(const PrimalCtx<T, V>& x, const IlTile& t,
+                                            const Stage<T>& st, double (&moved)[V]) {
+    const Interleaved<T>& il = *x.il;
+    const int warp = threadIdx.x >> 5;
+    const int64_t bp = il.bp;
+    for (int l0 = warp; l0 < t.lines; l0 += kU * kIlWarps) {
+        PrimalLine<T, V, kFam> L[kU];
+        T sum[kU][V];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int l = l0 + u * kIlWarps;
+            if (l < t.lines) primal_load(x, t.line0 + l, L[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int l = l0 + u * kIlWarps;
+            if (l >= t.lines) continue;
+            if (kStaged) {
+                gather_sum<2, T, V>(st.idx + st.ptr[l], st.val + st.ptr[l], st.ptr[l + 1] - st.ptr[l],
+                                    x.YR + x.col0, x.YW + x.col0, x.ls.fix, bp, sum[u]);
+            } else {
+                const int64_t k0 = __ldg(il.at_ptr + t.line0 + l), k1 = __ldg(il.at_ptr + t.line0 + l + 1);
+                gather_sum<2, T, V>(il.at_idx + k0, il.at_val + k0, static_cast<int>(k1 - k0),
+                                    x.YR + x.col0, x.YW + x.col0, x.ls.fix, bp, sum[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int l = l0 + u * kIlWarps;
+            if (l < t.lines) primal_store(x, t.line0 + l, L[u], sum[u], moved);
+        }
+    }
+}
+
+template <class T, int V, bool kFam>
+__global__ void __launch_bounds__(kIlThreads, 3) k_il_primal(Interleaved<T> il, InstanceCtl* ctl,
+                                                             int measure, int slot) {
+    constexpr int G = 32 * V;
+    __shared__ Stage<T> st[2];
+    const int group = blockIdx.y;
+    const int lane = threadIdx.x & 31;
+    const int R = slot & 1, W = R ^ 1;
+    PrimalCtx<T, V> x;
+    x.il = &il;
+    x.col0 = static_cast<int64_t>(group) * G + lane * V;
+    x.ls = lane_state<T, V>(il, ctl, static_cast<int>(x.col0), measure, R, true);
+    if (!__syncthreads_or(x.ls.active != 0)) return;
+    x.XR = il.X[R];
+    x.XW_read = il.X[W];
+    x.xr = il.X[R];
+    x.xw = il.X[W];
+    x.YR = il.Y[R];
+    x.YW = il.Y[W];
+    x.avg = il.avg_x;
+    x.fc = (il.family >> kIlC) & 1;
+    x.fl = (il.family >> kIlXl) & 1;
+    x.fu = (il.family >> kIlXu) & 1;
+
+    double moved[1][V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) moved[0][v] = 0.0;
+    const int t0 = il.at_cta[blockIdx.x], t1 = il.at_cta[blockIdx.x + 1];
+    if (t0 < t1) {
+        const IlTile first = il.at_tiles[t0];
+        if (first.staged) stage_tile_async(first, il.at_ptr, il.at_idx, il.at_val, st[0]);
+    }
+    for (int ti = t0; ti < t1; ++ti) {
+        const IlTile t = il.at_tiles[ti];
+        copy_async_wait();
+        __syncthreads();
+        if (ti + 1 < t1) {
+            const IlTile nt = il.at_tiles[ti + 1];
+            if (nt.staged) stage_tile_async(nt, il.at_ptr, il.at_idx, il.at_val, st[(ti + 1 - t0) & 1]);
+        }
+        if (t.staged) primal_tile<kPrimalU<T, V>, true, kFam>(x, t, st[(ti - t0) & 1], moved[0]);
+        else primal_tile<1, false, kFam>(x, t, st[0], moved[0]);
+        __syncthreads();
+    }
+    double cta[1];
+    cta_sums<1, V>(moved, cta);
+    // The partial only: the dual kernel's CTAs add the batches.
+    if (threadIdx.x < G)
+        il.part_primal[(static_cast<int64_t>(group) * il.col_ctas + blockIdx.x) * G + threadIdx.x] = cta[0];
+}
+
+// ---------------------------------------------------------------------------
+// Dual half and the trial decision
+// ---------------------------------------------------------------------------
+template <class T, int V>
+struct DualCtx {
+    const Interleaved<T>* il;
+    Lanes<T, V> ls;
+    const T* xt;       // trial x of the lane's instances
+    const T* YR;
+    const T* YW;
+    const T* AXR;
+    const T* AXW;
+    T* yr;
+    T* yw;
+    T* axr;
+    T* axw;
+    T* avg;
+    int64_t col0;
+    bool fl, fu;
+};
+
+template <class T, int V, bool kFam>
+struct DualLine {
+    T ax[V], prev[V], a[V];
+    Bounds<T, V, kFam> b;
+    T sg, isg;
+};
+
+template <class T, int V, bool kFam>
+__device__ __forceinline__ void dual_load(const DualCtx<T, V>& x, int i, DualLine<T, V, kFam>& L) {
+    const Interleaved<T>& il = *x.il;
+    const int64_t e = i * static_cast<int64_t>(il.bp) + x.col0;
+    L.sg = __ldg(il.sigma + i);
+    L.isg = __ldg(il.isigma + i);
+    load_committed<T, V>(x.AXR, x.AXW, e, x.ls.fix, L.ax);
+    load_committed<T, V>(x.YR, x.YW, e, x.ls.fix, L.prev);
+    load_bounds<T, V, kFam>(il, kIlRl, kIlRu, x.fl, x.fu, i, e, L.b);
+    if (x.ls.pending) ldv<T, V>(x.avg + e, L.a);
+}
+
+template <class T, int V, bool kFam>
+__device__ __forceinline__ void dual_store(const DualCtx<T, V>& x, int i, const DualLine<T, V, kFam>& L,
+                                           const T (&next)[V], double (&red)[2][V]) {
+    const Interleaved<T>& il = *x.il;
+    const int64_t e = i * static_cast<int64_t>(il.bp) + x.col0;
+    T upd[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const T dact = next[v] - L.ax[v];
+        const T ext = next[v] + dact;
+        const T step = smax(x.ls.step[v] * L.sg, min_dual_step<T>());
+        const T w = L.prev[v] + step * ext;
+        upd[v] = smax(w - step * L.b.h(v), T(0)) + smin(w - step * L.b.l(v), T(0));
+        const double d = static_cast<double>(upd[v] - L.prev[v]);
+        if ((x.ls.active >> v) & 1) {
+            red[0][v] += d * d * static_cast<double>(L.isg);
+            red[1][v] += d * static_cast<double>(dact);
+        }
+    }
+    stv_masked<T, V>(x.yw + e, upd, x.ls.active);
+    stv_masked<T, V>(x.axw + e, next, x.ls.active);
+    if (x.ls.pending) {
+        T a[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+            a[v] = ((x.ls.pending >> v) & 1) ? L.a[v] + x.ls.frac[v] * (L.prev[v] - L.a[v]) : L.a[v];
+        stv<T, V>(x.avg + e, a);
+    }
+    if (x.ls.fix) {
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+            if ((x.ls.fix >> v) & 1) {
+                x.yr[e + v] = L.prev[v];
+                x.axr[e + v] = L.ax[v];
+            }
+    }
+}
+
+template <int kU, bool kStaged, bool kFam, class T, int V>
+__device__ __forceinline__ void dual_tile(const DualCtx<T, V>& x, const IlTile& t, const Stage<T>& st,
+                                          double (&red)[2][V]) {
+    const Interleaved<T>& il = *x.il;
+    const int warp = threadIdx.x >> 5;
+    const int64_t bp = il.bp;
+    for (int l0 = warp; l0 < t.lines; l0 += kU * kIlWarps) {
+        DualLine<T, V, kFam> L[kU];
+        T sum[kU][V];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int l = l0 + u * kIlWarps;
+            if (l < t.lines) dual_load(x, t.line0 + l, L[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int l = l0 + u * kIlWarps;
+            if (l >= t.lines) continue;
+            if (kStaged) {
+                gather_sum<kDualGather<V>, T, V>(st.idx + st.ptr[l], st.val + st.ptr[l],
+                                                 st.ptr[l + 1] - st.ptr[l], x.xt, x.xt, 0u, bp, sum[u]);
+            } else {
+                const int64_t k0 = __ldg(il.a_ptr + t.line0 + l), k1 = __ldg(il.a_ptr + t.line0 + l + 1);
+                gather_sum<kDualGather<V>, T, V>(il.a_idx + k0, il.a_val + k0, static_cast<int>(k1 - k0),
+                                                 x.xt, x.xt, 0u, bp, sum[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int l = l0 + u * kIlWarps;
+            if (l < t.lines) dual_store(x, t.line0 + l, L[u], sum[u], red);
+        }
+    }
+}
+
+template <class T, int V, bool kFam>
+__global__ void __launch_bounds__(kIlThreads, 3) k_il_dual(Interleaved<T> il, InstanceCtl* ctl,
+                                                           DeviceOptions o, int measure, int slot) {
+    constexpr int G = 32 * V;
+    __shared__ Stage<T> st[2];
+    const int group = blockIdx.y;
+    const int lane = threadIdx.x & 31;
+    const int R = slot & 1, W = R ^ 1;
+    DualCtx<T, V> x;
+    x.il = &il;
+    x.col0 = static_cast<int64_t>(group) * G + lane * V;
+    x.ls = lane_state<T, V>(il, ctl, static_cast<int>(x.col0), measure, R, false);
+    if (!__syncthreads_or(x.ls.active != 0)) return;
+    x.xt = il.X[W] + x.col0;
+    x.YR = il.Y[R];
+    x.YW = il.Y[W];
+    x.AXR = il.AX[R];
+    x.AXW = il.AX[W];
+    x.yr = il.Y[R];
+    x.yw = il.Y[W];
+    x.axr = il.AX[R];
+    x.axw = il.AX[W];
+    x.avg = il.avg_y;
+    x.fl = (il.family >> kIlRl) & 1;
+    x.fu = (il.family >> kIlRu) & 1;
+
+    double red[2][V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) red[0][v] = red[1][v] = 0.0;
+    const int t0 = il.a_cta[blockIdx.x], t1 = il.a_cta[blockIdx.x + 1];
+    if (t0 < t1) {
+        const IlTile first = il.a_tiles[t0];
+        if (first.staged) stage_tile_async(first, il.a_ptr, il.a_idx, il.a_val, st[0]);
+    }
+    for (int ti = t0; ti < t1; ++ti) {
+        const IlTile t = il.a_tiles[ti];
+        copy_async_wait();
+        __syncthreads();
+        if (ti + 1 < t1) {
+            const IlTile nt = il.a_tiles[ti + 1];
+            if (nt.staged) stage_tile_async(nt, il.a_ptr, il.a_idx, il.a_val, st[(ti + 1 - t0) & 1]);
+        }
+        if (t.staged) dual_tile<kDualU<T, V>, true, kFam>(x, t, st[(ti - t0) & 1], red);
+        else dual_tile<1, false, kFam>(x, t, st[0], red);
+        __syncthreads();
+    }
+    double cta[2];
+    cta_sums<2, V>(red, cta);
+    if (measure) return;
+    const int64_t gp = static_cast<int64_t>(group);
+    const int t = threadIdx.x;
+    // The primal kernel's batch sums, spread over this kernel's CTAs.
+    if (t < G) {
+        const double* pp = il.part_primal + gp * il.col_ctas * G;
+        double* pp2 = il.part2_primal + gp * il.col_batches * G;
+        for (int k = blockIdx.x; k < il.col_batches; k += il.row_ctas) {
+            const int b0 = k * kIlBatch;
+            const int n = il.col_ctas - b0 < kIlBatch ? il.col_ctas - b0 : kIlBatch;
+            double sp[1];
+            sum_rows<1, G>(pp, b0, n, t, sp);
+            pp2[static_cast<int64_t>(k) * G + t] = sp[0];
+        }
+    }
+    int32_t* cnt = il.cnt_dual + gp * (il.row_batches + 1);
+    if (!batch_sums<2, G>(cta, il.part_dual + gp * il.row_ctas * 2 * G, il.part2_dual + gp * il.row_batches * 2 * G,
+                          cnt, il.row_ctas, blockIdx.x))
+        return;
+    if (!arrive_last_cta(cnt + il.row_batches, il.row_batches)) return;
+    // The linesearch decision of each instance of the group (one thread each).
+    const int b = static_cast<int>(gp * G) + t;
+    if (t >= G || b >= il.count) return;
+    InstanceCtl& c = ctl[b];
+    if (!trial_active<T>(c)) return;
+    double pm[1], dd[2];
+    sum_batches<1, G>(il.part2_primal + gp * il.col_batches * G, il.col_batches, t, pm);
+    sum_batches<2, G>(il.part2_dual + gp * il.row_batches * 2 * G, il.row_batches, t, dd);
+    const int before = c.parity;
+    trial_control(c, o, pm[0], dd[0], dd[1], il.n);
+    c.ibuf = c.parity != before ? W : R;
+}
+
+// ---------------------------------------------------------------------------
+// Transposes between the layouts, one 32-line x 32-instance tile per CTA
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_il_move(IlMove<T> mv) {
+    __shared__ T tile[32][33];
+    __shared__ int32_t sel[32], par[32], ib[32];
+    const int group = blockIdx.y;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    if (threadIdx.x < 32) {
+        const int b = group * 32 + tx;
+        int s = 0, p = 0, q = 0;
+        if (b < mv.count) {
+            const InstanceCtl& c = mv.ctl[b];
+            switch (mv.select) {
+                case kIlAll: s = 1; break;
+                case kIlMasked: s = mv.mask[b] != 0; break;
+                case kIlAtCheck: s = c.stage == kStageCheck; break;
+                default: s = c.il_sync != 0; break;
+            }
+            p = c.parity;
+            q = c.ibuf;
+        }
+        sel[tx] = s;
+        par[tx] = p;
+        ib[tx] = q;
+    }
+    __syncthreads();
+    int pi = 0;
+    while (pi + 1 < mv.pairs && static_cast<int>(blockIdx.x) >= mv.pair[pi + 1].tile0) ++pi;
+    const IlPair<T>& P = mv.pair[pi];
+    const int l0 = (static_cast<int>(blockIdx.x) - P.tile0) * 32;
+    const int64_t bp = mv.bp;
+    if (mv.to_planar) {
+        for (int r = ty; r < 32; r += 8) {
+            const int line = l0 + r;
+            T v = T(0);
+            if (line < P.lines && sel[tx])
+                v = P.il[P.by_ibuf ? ib[tx] : 0][line * bp + group * 32 + tx];
+            tile[r][tx] = v;
+        }
+        __syncthreads();
+        for (int r = ty; r < 32; r += 8) {
+            const int64_t b = group * 32 + r;
+            const int line = l0 + tx;
+            if (sel[r] && line < P.lines)
+                P.planar[P.by_parity ? par[r] : 0][b * P.lines + line] = tile[tx][r];
+        }
+    } else {
+        for (int r = ty; r < 32; r += 8) {
+            const int64_t b = group * 32 + r;
+            const int line = l0 + tx;
+            T v = T(0);
+            if (sel[r] && line < P.lines) v = P.planar[P.by_parity ? par[r] : 0][b * P.lines + line];
+            tile[tx][r] = v;
+        }
+        __syncthreads();
+        for (int r = ty; r < 32; r += 8) {
+            const int line = l0 + r;
+            if (line < P.lines && sel[tx]) P.il[P.by_ibuf ? ib[tx] : 0][line * bp + group * 32 + tx] = tile[r][tx];
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 32 && sel[tx]) {
+        InstanceCtl& c = mv.ctl[group * 32 + tx];
+        if (mv.select == kIlAtCheck) c.il_sync = 1;
+        if (mv.reset_ibuf) c.ibuf = 0;
+    }
+}
+
+template <class T>
+__global__ void k_il_scale(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                           const double* __restrict__ orig, T* __restrict__ val,
+                           const double* __restrict__ ls, const double* __restrict__ os,
+                           int32_t lines) {
+    const int line = blockIdx.x * blockDim.x + threadIdx.x;
+    if (line >= lines) return;
+    const double f = ls[line];
+    for (int64_t k = ptr[line]; k < ptr[line + 1]; ++k)   // SparseMatrix::scaled, sparse_matrix.cpp:243-274
+        val[k] = static_cast<T>(orig[k] * (f * os[idx[k]]));
+}
+
+__device__ __forceinline__ double il_scale_bound(double b, double f) { return isfinite(b) ? b * f : b; }
+
+struct FamSrc {
+    const double* v[kIlVecs];
+};
+
+template <class T>
+__global__ void k_il_family(Interleaved<T> il, FamSrc src, const double* __restrict__ rs,
+                            const double* __restrict__ cs) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < il.n) {   // scaling.cpp:109-135, as the per-instance setup scales them
+        const double f = cs[t];
+        il.fam[kIlC][t] = static_cast<T>(src.v[kIlC][t] * f);
+        il.fam[kIlXl][t] = static_cast<T>(il_scale_bound(src.v[kIlXl][t], 1.0 / f));
+        il.fam[kIlXu][t] = static_cast<T>(il_scale_bound(src.v[kIlXu][t], 1.0 / f));
+    }
+    if (t < il.m) {
+        const double f = rs[t];
+        il.fam[kIlRl][t] = static_cast<T>(il_scale_bound(src.v[kIlRl][t], f));
+        il.fam[kIlRu][t] = static_cast<T>(il_scale_bound(src.v[kIlRu][t], f));
+    }
+}
+
+}  // namespace
+
+template <class T, int V>
+int blocks_per_sm(bool dual) {
+    int r = 0;
+    if (dual) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_il_dual<T, V, false>, kIlThreads, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_il_primal<T, V, false>, kIlThreads, 0);
+    return r > 0 ? r : 1;
+}
+
+template <class T>
+int il_blocks_per_sm(int vl, bool dual) {
+    if constexpr (sizeof(T) == 4) {
+        if (vl == 4) return blocks_per_sm<T, 4>(dual);
+    }
+    if (vl == 2) return blocks_per_sm<T, 2>(dual);
+    return blocks_per_sm<T, 1>(dual);
+}
+
+namespace {
+
+constexpr int32_t kXBounds = (1 << kIlXl) | (1 << kIlXu);
+constexpr int32_t kRBounds = (1 << kIlRl) | (1 << kIlRu);
+
+template <class T, int V>
+void primal_v(const Interleaved<T>& il, InstanceCtl* ctl, int measure, int slot, cudaStream_t s) {
+    const dim3 grid(il.col_ctas, il.groups);
+    if ((il.family & kXBounds) == kXBounds)
+        k_il_primal<T, V, true><<<grid, kIlThreads, 0, s>>>(il, ctl, measure, slot);
+    else
+        k_il_primal<T, V, false><<<grid, kIlThreads, 0, s>>>(il, ctl, measure, slot);
+}
+
+template <class T, int V>
+void dual_v(const Interleaved<T>& il, InstanceCtl* ctl, const DeviceOptions& o, int measure, int slot,
+            cudaStream_t s) {
+    const dim3 grid(il.row_ctas, il.groups);
+    if ((il.family & kRBounds) == kRBounds)
+        k_il_dual<T, V, true><<<grid, kIlThreads, 0, s>>>(il, ctl, o, measure, slot);
+    else
+        k_il_dual<T, V, false><<<grid, kIlThreads, 0, s>>>(il, ctl, o, measure, slot);
+}
+
+}  // namespace
+
+template <class T>
+void launch_il_primal(const Interleaved<T>& il, InstanceCtl* ctl, int measure, int slot,
+                      cudaStream_t s) {
+    if constexpr (sizeof(T) == 4) {
+        if (il.vl == 4) return primal_v<T, 4>(il, ctl, measure, slot, s);
+    }
+    if (il.vl == 2) primal_v<T, 2>(il, ctl, measure, slot, s);
+    else primal_v<T, 1>(il, ctl, measure, slot, s);
+}
+
+template <class T>
+void launch_il_dual(const Interleaved<T>& il, InstanceCtl* ctl, const DeviceOptions& o,
+                    int measure, int slot, cudaStream_t s) {
+    if constexpr (sizeof(T) == 4) {
+        if (il.vl == 4) return dual_v<T, 4>(il, ctl, o, measure, slot, s);
+    }
+    if (il.vl == 2) dual_v<T, 2>(il, ctl, o, measure, slot, s);
+    else dual_v<T, 1>(il, ctl, o, measure, slot, s);
+}
+
+template <class T>
+void launch_il_move(const IlMove<T>& mv, int groups, cudaStream_t s) {
+    if (mv.pairs == 0 || mv.tiles == 0) return;
+    k_il_move<T><<<dim3(mv.tiles, groups), 256, 0, s>>>(mv);
+}
+
+template <class T>
+void launch_il_scale(const int64_t* ptr, const int32_t* idx, const double* orig, T* val,
+                     const double* line_scale, const double* other_scale, int32_t lines,
+                     cudaStream_t s) {
+    if (lines <= 0) return;
+    k_il_scale<T><<<(lines + 255) / 256, 256, 0, s>>>(ptr, idx, orig, val, line_scale, other_scale, lines);
+}
+
+template <class T>
+void launch_il_family(const Interleaved<T>& il, const double* const fam[kIlVecs],
+                      const double* rs, const double* cs, cudaStream_t s) {
+    FamSrc src;
+    for (int k = 0; k < kIlVecs; ++k) src.v[k] = fam[k];
+    const int len = il.n > il.m ? il.n : il.m;
+    if (len <= 0) return;
+    k_il_family<T><<<(len + 255) / 256, 256, 0, s>>>(il, src, rs, cs);
+}
+
+#define PDLPGPU_IL_INSTANTIATE(T)                                                                 \
+    template int il_blocks_per_sm<T>(int, bool);                                                         \
+    template void launch_il_primal<T>(const Interleaved<T>&, InstanceCtl*, int, int, cudaStream_t); \
+    template void launch_il_dual<T>(const Interleaved<T>&, InstanceCtl*, const DeviceOptions&, int, \
+                                    int, cudaStream_t);                                          \
+    template void launch_il_move<T>(const IlMove<T>&, int, cudaStream_t);                         \
+    template void launch_il_scale<T>(const int64_t*, const int32_t*, const double*, T*,           \
+                                     const double*, const double*, int32_t, cudaStream_t);        \
+    template void launch_il_family<T>(const Interleaved<T>&, const double* const*, const double*, \
+                                      const double*, cudaStream_t);
+PDLPGPU_IL_INSTANTIATE(float)
+PDLPGPU_IL_INSTANTIATE(double)
+
+}  // namespace pdlpgpu

@@ -180,15 +180,6 @@ __device__ __forceinline__ bool arrive_last(int32_t* counter, int expected) {
     return last != 0;
 }
 
-template <class T>
-__device__ __forceinline__ bool precision_matches(const InstanceCtl& c) {
-    return (c.fp64_stage != 0) == (sizeof(T) == 8);
-}
-
-template <class T>
-__device__ __forceinline__ bool trial_active(const InstanceCtl& c) {
-    return c.phase != kPhaseDone && c.stage == kStageTrial && precision_matches<T>(c);
-}
 
 __device__ __forceinline__ bool check_have_avg(const InstanceCtl& c, const DeviceOptions& o) {
     if (c.check_kind == kCheckInitial) return c.have_avg_at_check != 0;
@@ -199,9 +190,6 @@ template <class T> __device__ __forceinline__ const T* matrix_values(const Side&
 template <> __device__ __forceinline__ const double* matrix_values<double>(const Side& s) { return s.val_s64; }
 template <> __device__ __forceinline__ const float* matrix_values<float>(const Side& s) { return s.val_s32; }
 
-template <class T> __device__ __forceinline__ T min_dual_step();
-template <> __device__ __forceinline__ double min_dual_step<double>() { return 1e-300; }
-template <> __device__ __forceinline__ float min_dual_step<float>() { return 1e-37f; }
 
 // ---------------------------------------------------------------------------
 // Primal half (pdhg_kernel.cpp:47-104)
@@ -471,30 +459,12 @@ __global__ void __launch_bounds__(kThreads) k_check_prep(Global g, Work<T> w, De
 // ---------------------------------------------------------------------------
 // Check, matrix passes and decision
 // ---------------------------------------------------------------------------
-__device__ __noinline__ void check_control(const Global& g, const DeviceOptions& o, InstanceCtl& c,
-                              const InstanceInfo& inf) {
-    // Column-side and row-side elementwise partials.
-    double C[kPrepSlots], R[kPrepSlots], A3[3], T6[kCheckSlots];
-    for (int q = 0; q < kPrepSlots; ++q) { C[q] = 0.0; R[q] = 0.0; }
-    const int lane = threadIdx.x & 31;
-    for (int q = 0; q < kPrepSlots; ++q) {
-        double tc = 0.0, tr = 0.0;
-        for (int k = inf.vec_cta_begin + lane; k < inf.vec_cta_end; k += 32) {
-            const double v = g.part_prep[static_cast<int64_t>(k) * kPrepSlots + q];
-            if (g.vec[k].is_row) tr += v; else tc += v;
-        }
-        for (int s = 16; s > 0; s >>= 1) {
-            tc += __shfl_xor_sync(kFull, tc, s);
-            tr += __shfl_xor_sync(kFull, tr, s);
-        }
-        C[q] = tc;
-        R[q] = tr;
-    }
-    for (int q = 0; q < 3; ++q)
-        A3[q] = warp_range_sum(g.part_check, inf.a_cta_begin, inf.a_cta_end, kCheckSlots, q);
-    const int at0 = g.a.num_ctas + inf.at_cta_begin, at1 = g.a.num_ctas + inf.at_cta_end;
-    for (int q = 0; q < kCheckSlots; ++q) T6[q] = warp_range_sum(g.part_check, at0, at1, kCheckSlots, q);
-    if (lane != 0) return;
+// The decision of one check from its sums (pdlp_solver.cpp:239-476,
+// feasibility_polishing.cpp:107-141). C/R: column- and row-side elementwise
+// sums (kPrepSlots each), A3: row-pass sums, T6: column-pass sums.
+__device__ __noinline__ void check_decide(const DeviceOptions& o, InstanceCtl& c, int32_t n_cols,
+                                          const double* C, const double* R, const double* A3,
+                                          const double* T6) {
 
     c.pending_avg = 0;
     const bool have_avg = check_have_avg(c, o);
@@ -551,7 +521,7 @@ __device__ __noinline__ void check_control(const Global& g, const DeviceOptions&
             finish(c, 0, kMsgInitialOptimal, false);
             return;
         }
-        loop_top_main(c, o, inf.n);
+        loop_top_main(c, o, n_cols);
         return;
     }
 
@@ -635,7 +605,34 @@ __device__ __noinline__ void check_control(const Global& g, const DeviceOptions&
         c.since_restart = 0;
         ++c.restart_count;
     }
-    loop_top_main(c, o, inf.n);
+    loop_top_main(c, o, n_cols);
+}
+
+__device__ __noinline__ void check_control(const Global& g, const DeviceOptions& o, InstanceCtl& c,
+                              const InstanceInfo& inf) {
+    // Column-side and row-side elementwise partials.
+    double C[kPrepSlots], R[kPrepSlots], A3[3], T6[kCheckSlots];
+    for (int q = 0; q < kPrepSlots; ++q) { C[q] = 0.0; R[q] = 0.0; }
+    const int lane = threadIdx.x & 31;
+    for (int q = 0; q < kPrepSlots; ++q) {
+        double tc = 0.0, tr = 0.0;
+        for (int k = inf.vec_cta_begin + lane; k < inf.vec_cta_end; k += 32) {
+            const double v = g.part_prep[static_cast<int64_t>(k) * kPrepSlots + q];
+            if (g.vec[k].is_row) tr += v; else tc += v;
+        }
+        for (int s = 16; s > 0; s >>= 1) {
+            tc += __shfl_xor_sync(kFull, tc, s);
+            tr += __shfl_xor_sync(kFull, tr, s);
+        }
+        C[q] = tc;
+        R[q] = tr;
+    }
+    for (int q = 0; q < 3; ++q)
+        A3[q] = warp_range_sum(g.part_check, inf.a_cta_begin, inf.a_cta_end, kCheckSlots, q);
+    const int at0 = g.a.num_ctas + inf.at_cta_begin, at1 = g.a.num_ctas + inf.at_cta_end;
+    for (int q = 0; q < kCheckSlots; ++q) T6[q] = warp_range_sum(g.part_check, at0, at1, kCheckSlots, q);
+    if (lane != 0) return;
+    check_decide(o, c, inf.n, C, R, A3, T6);
 }
 
 template <int V>
@@ -824,6 +821,7 @@ __global__ void k_finalize(Global g, int32_t count, int32_t* active) {
     c.need_refresh = 0;
     c.to_polish = 0;
     c.save_ray = 0;
+    c.il_sync = 0;
 }
 
 // Mixed precision: the FP64 stage starts from the last FP32 restart point.

@@ -142,3 +142,37 @@ class FlowWarmStart:
         if rc != 0:
             raise RuntimeError(native.last_error())
         return wx, wy, ww
+
+
+def train_flow_model(graph, count: int, tol: float = 1e-4, precision: str = "mixed",
+                     slots: int = 1024, seed: int = 7, device: int = 0, epochs: int = 30,
+                     lr: float = 1e-3, lr_final: float = 1e-4, log=None):
+    """Solves `count` seeded instances of the flow family with the batched
+    engine (a stream through `slots` device slots, cold start, tolerance
+    `tol`), then fits a FlowWarmStart on their solutions. Returns (model,
+    info) with the timings and the final training loss."""
+    import time
+
+    from . import generators as g
+    from .lp import PdlpOptions
+    from .session import Session
+
+    supply, cost = g.flow_parameters(graph, count, seed=seed)
+    family = g.flow_lp(graph, supply[0], cost[0])
+    t0 = time.perf_counter()
+    S = Session(family, min(slots, count), PdlpOptions().with_tolerance(tol), precision=precision,
+                device=device)
+    out = S.stream(count, objective=cost, row_lower=supply, row_upper=supply)
+    S.close()
+    t1 = time.perf_counter()
+    ok = np.array([st == 0 for st in out["status"]])
+    model = FlowWarmStart(graph, device=device, seed=seed)
+    hist = model.fit(supply[ok], cost[ok], out["primal"][ok], out["dual"][ok],
+                     out["final_primal_weight"][ok], epochs=epochs, lr=lr, lr_final=lr_final,
+                     log=log)
+    t2 = time.perf_counter()
+    info = dict(instances=int(count), solved=int(ok.sum()), label_tolerance=tol,
+                label_precision=precision, label_seconds=round(t1 - t0, 2),
+                label_mean_iterations=float(out["iterations"].mean()),
+                train_seconds=round(t2 - t1, 2), epochs=epochs, final_loss=float(hist[-1]))
+    return model, info

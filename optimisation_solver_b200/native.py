@@ -57,7 +57,7 @@ class ExtOptions(C.Structure):
                 ("vector_width", C.c_int32), ("chunk_slack", C.c_int32),
                 ("fp32_stall_checks", C.c_int32), ("fp32_switch_factor", C.c_int32),
                 ("disable_graphs", C.c_int32), ("cta_slots", C.c_int32),
-                ("reserved", C.c_int32 * 7)]
+                ("layout", C.c_int32), ("lane_instances", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class WarmStart(C.Structure):
@@ -114,6 +114,7 @@ SIGNATURES = {
     "pdlpgpu_session_stream": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64] + [C.c_void_p] * 10 +
                                [_i32p, _i64p, _dp]),
     "pdlpgpu_session_time_kernels": (C.c_int32, [C.c_void_p, C.c_int32, _dp]),
+    "pdlpgpu_session_loop_timing": (C.c_int32, [C.c_void_p, _dp]),
     "pdlpgpu_mlp_create": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
                                        C.c_int32, C.POINTER(C.c_void_p)]),
     "pdlpgpu_mlp_destroy": (None, [C.c_void_p]),

@@ -15,6 +15,7 @@ from . import native
 from .lp import CompiledLp, PdlpOptions, PdlpStatus
 
 _PRECISIONS = {"fp64": 0, "mixed": 1}
+_LAYOUTS = {"auto": 0, "sell": 1, "interleaved": 2}
 
 
 def _addr(a):
@@ -30,13 +31,17 @@ def _addr(a):
 
 class Session:
     def __init__(self, family: CompiledLp, batch: int, options: PdlpOptions | None = None,
-                 precision: str = "fp64", device: int = 0, **tuning):
+                 precision: str = "fp64", device: int = 0, layout: str = "auto", **tuning):
+        """`layout`: "interleaved" keeps the trial kernels' vectors as
+        [line][instance] so a warp serves 32 instances; "sell" walks the
+        matrix once per instance; "auto" picks interleaved from 16 instances."""
         self.family = family
         self.batch = int(batch)
         self.n, self.m = family.num_cols, family.num_rows
         self._h = native.LpHandle(family)
         self._o = native.options_struct(options or PdlpOptions())
-        self._e = native.ext_struct(precision=_PRECISIONS[precision], device=device, **tuning)
+        self._e = native.ext_struct(precision=_PRECISIONS[precision], device=device,
+                                    layout=_LAYOUTS[layout], **tuning)
         self._s = C.c_void_p()
         rc = native.lib().pdlpgpu_session_create(C.byref(self._h.struct), self.batch,
                                                  C.byref(self._o), C.byref(self._e),
@@ -130,6 +135,16 @@ class Session:
         s, n = C.c_double(), C.c_int64()
         native.lib().pdlpgpu_session_last_timing(self._s, C.byref(s), C.byref(n))
         return s.value, n.value
+
+    def loop_timing(self) -> dict:
+        """Live durations of the last solve or stream, from CUDA events
+        recorded inside the captured iteration loop (one trial per chunk)."""
+        out = np.zeros(15)
+        if native.lib().pdlpgpu_session_loop_timing(self._s, native.ptr(out)) != 0:
+            raise RuntimeError("loop_timing failed")
+        return dict(primal_ms=out[0], dual_ms=out[1], samples=int(out[2]), chunk_ms=out[3],
+                    chunks=int(out[4]), loop_seconds=out[5], check_ms=out[6],
+                    by_slot=[(out[7 + 2 * k], out[8 + 2 * k]) for k in range(4)])
 
     def time_kernels(self, reps: int = 20) -> dict:
         out = np.zeros(6)
