@@ -22,6 +22,7 @@
 //     them in a fixed order. Runs are therefore bitwise reproducible.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 
 namespace pdlpgpu {
@@ -64,15 +65,23 @@ struct InstanceInfo {
 };
 
 // Per-instance scalar state of the solve; one writer at a time (the last CTA
-// of the instance in the kernel that owns the decision).
-struct InstanceCtl {
-    // --- control flow
+// of the instance in the kernel that owns the decision). The first 64 bytes
+// hold what every trial kernel reads at entry, so it is fetched with three
+// 16-byte loads.
+struct alignas(64) InstanceCtl {
+    // --- hot block (64 bytes)
+    double trial_eta, trial_omega;   // step and weight of the next trial
+    double avg_frac;                 // fraction owed by the pending update
     int32_t phase;          // kPhaseMain / kPhasePolish / kPhaseDone
     int32_t stage;          // kStageTrial / kStageCheck
-    int32_t check_kind;     // kCheckInitial / kCheckMain / kCheckPolish
-    int32_t parity;         // current iterate lives in buffer [parity]
     int32_t pending_avg;    // average update owed for the current iterate
+    int32_t fp64_stage;     // mixed solves: 1 once the FP64 stage has started
+    int32_t ibuf;           // interleaved layout: buffer holding the committed iterate
+    int32_t parity;         // current iterate lives in buffer [parity]
+    int32_t check_kind;     // kCheckInitial / kCheckMain / kCheckPolish
     int32_t trials_this_iter;
+    int32_t hot_pad[2];
+    // --- control flow
     int32_t status;         // final status once phase == done
     int32_t message;        // message id
     int32_t restart_count;
@@ -86,10 +95,9 @@ struct InstanceCtl {
     int32_t to_polish;      // load best point into the iterate, in working coordinates
     int32_t save_ray;       // copy the ray scratch to the ray buffers
     int32_t have_avg_at_check;
-    int32_t fp64_stage;     // mixed solves: 1 once the FP64 stage has started
     int32_t stall_checks;
-    int32_t ibuf;           // interleaved layout: buffer holding the committed iterate
     int32_t il_sync;        // interleaved layout: the iterate was copied out for a check
+    int32_t pad0;
     // --- counters
     int64_t iteration;       // main phase: committed iterations (state.iteration)
     int64_t step_trials;     // main phase trials
@@ -104,10 +112,8 @@ struct InstanceCtl {
     // --- step control (main controller, polishing controller, trial step)
     double eta, omega, eta_max;
     double ctl_eta, ctl_omega;
-    double trial_eta, trial_omega;
     // --- averaging
     double avg_weight;       // total weight W
-    double avg_frac;         // fraction owed by the pending update
     // --- restart state
     double restart_baseline;
     double prev_candidate;
@@ -121,6 +127,9 @@ struct InstanceCtl {
     // --- last trial reductions and ray verdicts (diagnostics and component tests)
     double dbg[12];
 };
+
+static_assert(offsetof(InstanceCtl, hot_pad) + 8 == 64, "hot block of InstanceCtl is 64 bytes");
+static_assert(offsetof(InstanceCtl, ibuf) == 40, "trial kernels read the hot block by offset");
 
 enum : int32_t { kPhaseMain = 0, kPhasePolish = 1, kPhaseDone = 2 };
 enum : int32_t { kStageTrial = 0, kStageCheck = 1 };

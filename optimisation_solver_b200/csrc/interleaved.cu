@@ -76,6 +76,36 @@ __device__ __forceinline__ void stv(T* p, const T (&o)[V]) {
     }
 }
 
+// Use-once streams (evict-first in L2), so that the trial point, which the
+// dual gathers next and the following primal reads, stays resident.
+template <class T, int V>
+__device__ __forceinline__ void ldv_cs(const T* p, T (&o)[V]) {
+    if constexpr (V == 1) {
+        o[0] = __ldcs(p);
+    } else if constexpr (V == 2) {
+        const auto v = __ldcs(reinterpret_cast<const typename Pack<T, 2>::type*>(p));
+        o[0] = v.x; o[1] = v.y;
+    } else {
+        const auto v = __ldcs(reinterpret_cast<const typename Pack<T, 4>::type*>(p));
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    }
+}
+
+template <class T, int V>
+__device__ __forceinline__ void stv_cs(T* p, const T (&o)[V]) {
+    if constexpr (V == 1) {
+        __stcs(p, o[0]);
+    } else if constexpr (V == 2) {
+        typename Pack<T, 2>::type v;
+        v.x = o[0]; v.y = o[1];
+        __stcs(reinterpret_cast<typename Pack<T, 2>::type*>(p), v);
+    } else {
+        typename Pack<T, 4>::type v;
+        v.x = o[0]; v.y = o[1]; v.z = o[2]; v.w = o[3];
+        __stcs(reinterpret_cast<typename Pack<T, 4>::type*>(p), v);
+    }
+}
+
 // Stores the active elements only (all of them with one access when every
 // instance of the lane is active): an idle instance's buffer may hold its
 // committed point.
@@ -100,25 +130,62 @@ struct Lanes {
     T step[V];          // eta / omega (primal) or eta * omega (dual)
 };
 
+// The hot block of an instance's control (the fields at its head, laid out
+// by InstanceCtl) in three independent 16-byte loads.
+struct HotCtl {
+    double eta, omega, frac;
+    int32_t phase, stage, pending, fp64, ibuf;
+};
+
+__device__ __forceinline__ HotCtl load_hot(const InstanceCtl* c) {
+    const int4* p = reinterpret_cast<const int4*>(c);
+    const int4 a = p[0], b = p[1], d = p[2];
+    HotCtl h;
+    h.eta = __hiloint2double(a.y, a.x);
+    h.omega = __hiloint2double(a.w, a.z);
+    h.frac = __hiloint2double(b.y, b.x);
+    h.phase = b.z;
+    h.stage = b.w;
+    h.pending = d.x;
+    h.fp64 = d.y;
+    h.ibuf = d.z;
+    return h;
+}
+
+// The lane's instances' state. Every warp of a CTA serves the same
+// instances, so warp 0 alone reads their control blocks (one L2 request per
+// block per CTA instead of one per warp: hundreds of CTAs read the same few
+// hundred blocks at kernel entry) and shares them through `hot` (G entries
+// of shared memory). Contains a CTA-wide barrier.
 template <class T, int V>
 __device__ __forceinline__ Lanes<T, V> lane_state(const Interleaved<T>& il, const InstanceCtl* ctl,
-                                                  int first, int measure, int R, bool primal) {
+                                                  int first, int measure, int R, bool primal,
+                                                  HotCtl* hot) {
     Lanes<T, V> s{0u, 0u, 0u, {}, {}};
+    const int lane = threadIdx.x & 31;
+    if ((threadIdx.x >> 5) == 0) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const int b = first + v < il.count ? first + v : il.count - 1;
+            hot[lane * V + v] = load_hot(ctl + b);
+        }
+    }
+    __syncthreads();
 #pragma unroll
     for (int v = 0; v < V; ++v) {
+        const HotCtl h = hot[lane * V + v];
         s.frac[v] = T(0);
         s.step[v] = T(0);
-        const int b = first + v;
-        if (b >= il.count) continue;
-        const InstanceCtl& c = ctl[b];
-        const bool act = measure ? true : trial_active<T>(c);
+        const bool exists = first + v < il.count;
+        const bool act = exists && (measure || (h.phase != kPhaseDone && h.stage == kStageTrial &&
+                                                (h.fp64 != 0) == (sizeof(T) == 8)));
         if (!act) continue;
         s.active |= 1u << v;
-        s.step[v] = static_cast<T>(primal ? c.trial_eta / c.trial_omega : c.trial_eta * c.trial_omega);
+        s.step[v] = static_cast<T>(primal ? h.eta / h.omega : h.eta * h.omega);
         if (measure) continue;
-        if (c.pending_avg) s.pending |= 1u << v;
-        s.frac[v] = static_cast<T>(c.avg_frac);
-        if (c.ibuf != R) s.fix |= 1u << v;
+        if (h.pending) s.pending |= 1u << v;
+        s.frac[v] = static_cast<T>(h.frac);
+        if (h.ibuf != R) s.fix |= 1u << v;
     }
     return s;
 }
@@ -368,9 +435,10 @@ __device__ __forceinline__ void primal_load(const PrimalCtx<T, V>& x, int j, Pri
     L.tj = __ldg(il.tau + j);
     L.itj = __ldg(il.itau + j);
     load_committed<T, V>(x.XR, x.XW_read, e, x.ls.fix, L.prev);
-    load_vec<T, V>(il, kIlC, x.fc, j, e, L.c);
+    if (x.fc) load_vec<T, V>(il, kIlC, true, j, e, L.c);
+    else ldv_cs<T, V>(il.vec[kIlC] + e, L.c);
     load_bounds<T, V, kFam>(il, kIlXl, kIlXu, x.fl, x.fu, j, e, L.b);
-    if (x.ls.pending) ldv<T, V>(x.avg + e, L.a);
+    if (x.ls.pending) ldv_cs<T, V>(x.avg + e, L.a);
 }
 
 template <class T, int V, bool kFam>
@@ -392,7 +460,7 @@ __device__ __forceinline__ void primal_store(const PrimalCtx<T, V>& x, int j, co
 #pragma unroll
         for (int v = 0; v < V; ++v)
             a[v] = ((x.ls.pending >> v) & 1) ? L.a[v] + x.ls.frac[v] * (L.prev[v] - L.a[v]) : L.a[v];
-        stv<T, V>(x.avg + e, a);
+        stv_cs<T, V>(x.avg + e, a);
     }
     if (x.ls.fix) {
 #pragma unroll
@@ -443,13 +511,14 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_primal(Interleaved<T> il, 
                                                              int measure, int slot) {
     constexpr int G = 32 * V;
     __shared__ Stage<T> st[2];
+    __shared__ HotCtl hot[G];
     const int group = blockIdx.y;
     const int lane = threadIdx.x & 31;
     const int R = slot & 1, W = R ^ 1;
     PrimalCtx<T, V> x;
     x.il = &il;
     x.col0 = static_cast<int64_t>(group) * G + lane * V;
-    x.ls = lane_state<T, V>(il, ctl, static_cast<int>(x.col0), measure, R, true);
+    x.ls = lane_state<T, V>(il, ctl, static_cast<int>(x.col0), measure, R, true, hot);
     if (!__syncthreads_or(x.ls.active != 0)) return;
     x.XR = il.X[R];
     x.XW_read = il.X[W];
@@ -607,13 +676,14 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_dual(Interleaved<T> il, In
                                                            DeviceOptions o, int measure, int slot) {
     constexpr int G = 32 * V;
     __shared__ Stage<T> st[2];
+    __shared__ HotCtl hot[G];
     const int group = blockIdx.y;
     const int lane = threadIdx.x & 31;
     const int R = slot & 1, W = R ^ 1;
     DualCtx<T, V> x;
     x.il = &il;
     x.col0 = static_cast<int64_t>(group) * G + lane * V;
-    x.ls = lane_state<T, V>(il, ctl, static_cast<int>(x.col0), measure, R, false);
+    x.ls = lane_state<T, V>(il, ctl, static_cast<int>(x.col0), measure, R, false, hot);
     if (!__syncthreads_or(x.ls.active != 0)) return;
     x.xt = il.X[W] + x.col0;
     x.YR = il.Y[R];
@@ -670,6 +740,11 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_dual(Interleaved<T> il, In
                           cnt, il.row_ctas, blockIdx.x))
         return;
     if (!arrive_last_cta(cnt + il.row_batches, il.row_batches)) return;
+    // The options by reference from shared memory: a reference to the kernel
+    // parameter would make every thread of every CTA copy it to local memory.
+    __shared__ DeviceOptions so;
+    if (t == 0) so = o;
+    __syncthreads();
     // The linesearch decision of each instance of the group (one thread each).
     const int b = static_cast<int>(gp * G) + t;
     if (t >= G || b >= il.count) return;
@@ -679,7 +754,7 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_dual(Interleaved<T> il, In
     sum_batches<1, G>(il.part2_primal + gp * il.col_batches * G, il.col_batches, t, pm);
     sum_batches<2, G>(il.part2_dual + gp * il.row_batches * 2 * G, il.row_batches, t, dd);
     const int before = c.parity;
-    trial_control(c, o, pm[0], dd[0], dd[1], il.n);
+    trial_control(c, so, pm[0], dd[0], dd[1], il.n);
     c.ibuf = c.parity != before ? W : R;
 }
 

@@ -323,11 +323,16 @@ __global__ void __launch_bounds__(kThreads, 6) k_dual(Global g, Work<T> w, Devic
     }
     if (g.measure) return;
     if (!arrive_last(g.count_dual + cw.instance, inf.a_cta_end - inf.a_cta_begin)) return;
+    // Options by reference from shared memory (a reference to the kernel
+    // parameter would copy it to local memory in every thread).
+    __shared__ DeviceOptions so;
+    if (threadIdx.x == 0) so = o;
+    __syncthreads();
     if (threadIdx.x < 32) {
         const double pm = warp_range_sum(g.part_primal, inf.at_cta_begin, inf.at_cta_end, 1, 0);
         const double dmv = warp_range_sum(g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 0);
         const double it = warp_range_sum(g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 1);
-        if (threadIdx.x == 0) trial_control(c, o, pm, dmv, it, inf.n);
+        if (threadIdx.x == 0) trial_control(c, so, pm, dmv, it, inf.n);
     }
 }
 
@@ -739,7 +744,10 @@ __global__ void __launch_bounds__(kThreads) k_check_spmv(Global g, DeviceOptions
     }
     const int expected = (inf.a_cta_end - inf.a_cta_begin) + (inf.at_cta_end - inf.at_cta_begin);
     if (!arrive_last(g.count_check + cw.instance, expected)) return;
-    if (threadIdx.x < 32) check_control(g, o, c, inf);
+    __shared__ DeviceOptions so;   // see k_dual
+    if (threadIdx.x == 0) so = o;
+    __syncthreads();
+    if (threadIdx.x < 32) check_control(g, so, c, inf);
 }
 
 // ---------------------------------------------------------------------------
