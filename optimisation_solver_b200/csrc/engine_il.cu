@@ -28,8 +28,14 @@ std::vector<int32_t> balanced_ranges(const std::vector<int64_t>& ptr, int32_t li
 
 // Tiles of every CTA's line range (tiles never cross a CTA boundary); fills
 // `cta_tiles` with the tile range of each CTA.
+int32_t line_segments(int64_t len) {
+    return static_cast<int32_t>((len + kIlSegEntries - 1) / kIlSegEntries);
+}
+
+// With `segmented`, a staged tile also holds at most kIlTileSegs row segments
+// (a row with more forms an unstaged tile of its own).
 std::vector<IlTile> make_tiles(const std::vector<int64_t>& ptr, const std::vector<int32_t>& cta_lines,
-                               std::vector<int32_t>& cta_tiles) {
+                               std::vector<int32_t>& cta_tiles, bool segmented) {
     std::vector<IlTile> tiles;
     const size_t ctas = cta_lines.size() - 1;
     cta_tiles.assign(ctas + 1, 0);
@@ -41,15 +47,22 @@ std::vector<IlTile> make_tiles(const std::vector<int64_t>& ptr, const std::vecto
             IlTile t{};
             t.line0 = i;
             t.e0 = ptr[static_cast<size_t>(i)];
-            if (ptr[static_cast<size_t>(i) + 1] - t.e0 > kIlTileEntries) {
+            const int64_t len = ptr[static_cast<size_t>(i) + 1] - t.e0;
+            if (len > kIlTileEntries || (segmented && line_segments(len) > kIlTileSegs)) {
                 t.lines = 1;
                 t.entries = static_cast<int32_t>(std::min<int64_t>(ptr[static_cast<size_t>(i) + 1] - t.e0, INT32_MAX));
                 t.staged = 0;
                 ++i;
             } else {
+                int32_t segs = 0;
                 while (i < end && i - t.line0 < kIlTileLines &&
-                       ptr[static_cast<size_t>(i) + 1] - t.e0 <= kIlTileEntries)
+                       ptr[static_cast<size_t>(i) + 1] - t.e0 <= kIlTileEntries) {
+                    const int64_t li = ptr[static_cast<size_t>(i) + 1] - ptr[static_cast<size_t>(i)];
+                    if (segmented && (line_segments(li) > kIlTileSegs || segs + line_segments(li) > kIlTileSegs))
+                        break;
+                    segs += line_segments(li);
                     ++i;
+                }
                 t.lines = i - t.line0;
                 t.entries = static_cast<int32_t>(ptr[static_cast<size_t>(i)] - t.e0);
                 t.staged = 1;
@@ -136,8 +149,16 @@ bool Engine::il_build(Interleaved<T>& il, const Work<T>& w) {
     il.row_ctas = std::max(1, std::min(row_target, (m + 7) / 8));
     il.col_ctas = std::max(1, std::min(col_target, (n + 7) / 8));
     std::vector<int32_t> a_cta, at_cta;
-    const std::vector<IlTile> a_tiles = make_tiles(ap, balanced_ranges(ap, m, il.row_ctas), a_cta);
-    const std::vector<IlTile> at_tiles = make_tiles(tp, balanced_ranges(tp, n, il.col_ctas), at_cta);
+    const std::vector<IlTile> a_tiles = make_tiles(ap, balanced_ranges(ap, m, il.row_ctas), a_cta, true);
+    const std::vector<IlTile> at_tiles = make_tiles(tp, balanced_ranges(tp, n, il.col_ctas), at_cta, false);
+    std::vector<int32_t> lseg(static_cast<size_t>(m) + 1, 0);
+    std::vector<int64_t> segstart;
+    for (int32_t r = 0; r < m; ++r) {
+        for (int64_t q = ap[static_cast<size_t>(r)]; q < ap[static_cast<size_t>(r) + 1]; q += kIlSegEntries)
+            segstart.push_back(q);
+        lseg[static_cast<size_t>(r) + 1] = static_cast<int32_t>(segstart.size());
+    }
+    segstart.push_back(ap[static_cast<size_t>(m)]);
 
     auto dalloc = [&](auto*& p, size_t count) {
         void* q = nullptr;
@@ -152,6 +173,8 @@ bool Engine::il_build(Interleaved<T>& il, const Work<T>& w) {
     int64_t *d_ap = nullptr, *d_tp = nullptr;
     int32_t *d_ai = nullptr, *d_ti = nullptr, *d_acta = nullptr, *d_atcta = nullptr;
     IlTile *d_atiles = nullptr, *d_attiles = nullptr;
+    int32_t* d_lseg = nullptr;
+    int64_t* d_segstart = nullptr;
     double *d_av = nullptr, *d_tv = nullptr;
     T *d_aval = nullptr, *d_tval = nullptr;
     const size_t nb = static_cast<size_t>(n) * il.bp, mb = static_cast<size_t>(m) * il.bp;
@@ -159,7 +182,8 @@ bool Engine::il_build(Interleaved<T>& il, const Work<T>& w) {
               dalloc(d_ti, ti.size()) && dalloc(d_av, av.size()) && dalloc(d_tv, tv.size()) &&
               dalloc(d_aval, av.size()) && dalloc(d_tval, tv.size()) && dalloc(d_acta, a_cta.size()) &&
               dalloc(d_atcta, at_cta.size()) && dalloc(d_atiles, a_tiles.size()) &&
-              dalloc(d_attiles, at_tiles.size());
+              dalloc(d_attiles, at_tiles.size()) && dalloc(d_lseg, lseg.size()) &&
+              dalloc(d_segstart, segstart.size());
     for (int b = 0; ok && b < 2; ++b)
         ok = dalloc(il.X[b], nb) && dalloc(il.Y[b], mb) && dalloc(il.AX[b], mb);
     ok = ok && dalloc(il.avg_x, nb) && dalloc(il.avg_y, mb);
@@ -180,7 +204,8 @@ bool Engine::il_build(Interleaved<T>& il, const Work<T>& w) {
          up(d_av, av.data(), av.size() * 8) && up(d_tv, tv.data(), tv.size() * 8) &&
          up(d_acta, a_cta.data(), a_cta.size() * 4) && up(d_atcta, at_cta.data(), at_cta.size() * 4) &&
          up(d_atiles, a_tiles.data(), a_tiles.size() * sizeof(IlTile)) &&
-         up(d_attiles, at_tiles.data(), at_tiles.size() * sizeof(IlTile));
+         up(d_attiles, at_tiles.data(), at_tiles.size() * sizeof(IlTile)) &&
+         up(d_lseg, lseg.data(), lseg.size() * 4) && up(d_segstart, segstart.data(), segstart.size() * 8);
     for (int b = 0; ok && b < 2; ++b)
         ok = check(cudaMemsetAsync(il.X[b], 0, nb * sizeof(T), stream_), "memset") &&
              check(cudaMemsetAsync(il.Y[b], 0, mb * sizeof(T), stream_), "memset") &&
@@ -199,6 +224,8 @@ bool Engine::il_build(Interleaved<T>& il, const Work<T>& w) {
     il.at_cta = d_atcta;
     il.a_tiles = d_atiles;
     il.at_tiles = d_attiles;
+    il.a_lseg = d_lseg;
+    il.a_segstart = d_segstart;
     // Scales and preconditioner are functions of A: instance 0's copies serve
     // every instance.
     launch_il_scale<T>(d_ap, d_ai, d_av, d_aval, g_.rs, g_.cs, m, stream_);

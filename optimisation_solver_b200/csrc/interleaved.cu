@@ -636,54 +636,100 @@ __device__ __forceinline__ void dual_store(const DualCtx<T, V>& x, int i, const 
     }
 }
 
-template <int kU, bool kStaged, bool kFam, class T, int V>
-__device__ __forceinline__ void dual_tile(const DualCtx<T, V>& x, const IlTile& t, const Stage<T>& st,
-                                          double (&red)[2][V]) {
-    const Interleaved<T>& il = *x.il;
-    const int warp = threadIdx.x >> 5;
-    const int64_t bp = il.bp;
-    for (int l0 = warp; l0 < t.lines; l0 += kU * kIlWarps) {
-        DualLine<T, V, kFam> L[kU];
-        T sum[kU][V];
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int l = l0 + u * kIlWarps;
-            if (l < t.lines) dual_load(x, t.line0 + l, L[u]);
-        }
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int l = l0 + u * kIlWarps;
-            if (l >= t.lines) continue;
-            if (kStaged) {
-                gather_sum<kDualGather<V>, T, V>(st.idx + st.ptr[l], st.val + st.ptr[l],
-                                                 st.ptr[l + 1] - st.ptr[l], x.xt, x.xt, 0u, bp, sum[u]);
-            } else {
-                const int64_t k0 = __ldg(il.a_ptr + t.line0 + l), k1 = __ldg(il.a_ptr + t.line0 + l + 1);
-                gather_sum<kDualGather<V>, T, V>(il.a_idx + k0, il.a_val + k0, static_cast<int>(k1 - k0),
-                                                 x.xt, x.xt, 0u, bp, sum[u]);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int l = l0 + u * kIlWarps;
-            if (l < t.lines) dual_store(x, t.line0 + l, L[u], sum[u], red);
-        }
+// Shared memory of the dual: one staged row tile, its segment table and the
+// per-segment partial sums of the lane's V instances.
+template <class T, int V>
+struct DualStage {
+    int32_t ptr[kIlTileLines + 1];
+    int32_t lseg[kIlTileLines + 1];      // line l: segments lseg[l] .. lseg[l + 1] - 1
+    int32_t segb[kIlTileSegs + 1];       // segment q: entries segb[q] .. segb[q + 1] - 1
+    int32_t idx[kIlTileEntries];
+    T val[kIlTileEntries];
+    T part[kIlTileSegs][32 * V];
+};
+
+template <class T, int V>
+__device__ __forceinline__ void stage_row_tile(const Interleaved<T>& il, const IlTile& t,
+                                               DualStage<T, V>& st) {
+    for (int q = threadIdx.x; q < t.entries; q += blockDim.x) {
+        copy_async<4>(st.idx + q, il.a_idx + t.e0 + q);
+        copy_async<sizeof(T)>(st.val + q, il.a_val + t.e0 + q);
     }
+    copy_async_commit();
+    const int32_t s0 = __ldg(il.a_lseg + t.line0);
+    const int32_t segs = __ldg(il.a_lseg + t.line0 + t.lines) - s0;
+    for (int q = threadIdx.x; q <= t.lines; q += blockDim.x) {
+        st.ptr[q] = static_cast<int32_t>(__ldg(il.a_ptr + t.line0 + q) - t.e0);
+        st.lseg[q] = __ldg(il.a_lseg + t.line0 + q) - s0;
+    }
+    for (int q = threadIdx.x; q <= segs; q += blockDim.x)
+        st.segb[q] = static_cast<int32_t>(__ldg(il.a_segstart + s0 + q) - t.e0);
+}
+
+// A staged row tile in two passes: every warp gathers whole segments (all of
+// a segment's entries in flight at once) into shared memory; then each row
+// adds its segments in order and takes its dual step.
+template <bool kFam, class T, int V>
+__device__ __forceinline__ void dual_tile_segmented(const DualCtx<T, V>& x, const IlTile& t,
+                                                    DualStage<T, V>& st, double (&red)[2][V]) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t bp = x.il->bp;
+    const int segs = st.lseg[t.lines];
+    for (int q = warp; q < segs; q += kIlWarps) {
+        const int b0 = st.segb[q];
+        T sum[V];
+        gather_sum<kIlSegEntries, T, V>(st.idx + b0, st.val + b0, st.segb[q + 1] - b0, x.xt, x.xt, 0u,
+                                        bp, sum);
+#pragma unroll
+        for (int v = 0; v < V; ++v) st.part[q][lane * V + v] = sum[v];
+    }
+    __syncthreads();
+    for (int l = warp; l < t.lines; l += kIlWarps) {
+        DualLine<T, V, kFam> L;
+        dual_load(x, t.line0 + l, L);
+        T next[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) next[v] = T(0);
+        for (int q = st.lseg[l]; q < st.lseg[l + 1]; ++q)
+#pragma unroll
+            for (int v = 0; v < V; ++v) next[v] += st.part[q][lane * V + v];
+        dual_store(x, t.line0 + l, L, next, red);
+    }
+}
+
+// A row too long to stage: warp 0 reads its entries from global memory.
+template <bool kFam, class T, int V>
+__device__ __forceinline__ void dual_line_global(const DualCtx<T, V>& x, const IlTile& t,
+                                                 double (&red)[2][V]) {
+    const Interleaved<T>& il = *x.il;
+    if ((threadIdx.x >> 5) != 0) return;
+    DualLine<T, V, kFam> L;
+    dual_load(x, t.line0, L);
+    const int64_t k0 = __ldg(il.a_ptr + t.line0), k1 = __ldg(il.a_ptr + t.line0 + 1);
+    T sum[V];
+    gather_sum<kDualGather<V>, T, V>(il.a_idx + k0, il.a_val + k0, static_cast<int>(k1 - k0), x.xt, x.xt,
+                                     0u, il.bp, sum);
+    dual_store(x, t.line0, L, sum, red);
 }
 
 template <class T, int V, bool kFam>
 __global__ void __launch_bounds__(kIlThreads, 3) k_il_dual(Interleaved<T> il, InstanceCtl* ctl,
                                                            DeviceOptions o, int measure, int slot) {
     constexpr int G = 32 * V;
-    __shared__ Stage<T> st[2];
-    __shared__ HotCtl hot[G];
+    // The lane states are read before the first tile is staged (the barrier
+    // in lane_state orders them), so they share the stage's memory.
+    __shared__ union Smem {
+        DualStage<T, V> st;
+        HotCtl hot[G];
+    } sm;
+    DualStage<T, V>& st = sm.st;
     const int group = blockIdx.y;
     const int lane = threadIdx.x & 31;
     const int R = slot & 1, W = R ^ 1;
     DualCtx<T, V> x;
     x.il = &il;
     x.col0 = static_cast<int64_t>(group) * G + lane * V;
-    x.ls = lane_state<T, V>(il, ctl, static_cast<int>(x.col0), measure, R, false, hot);
+    x.ls = lane_state<T, V>(il, ctl, static_cast<int>(x.col0), measure, R, false, sm.hot);
     if (!__syncthreads_or(x.ls.active != 0)) return;
     x.xt = il.X[W] + x.col0;
     x.YR = il.Y[R];
@@ -702,20 +748,16 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_dual(Interleaved<T> il, In
 #pragma unroll
     for (int v = 0; v < V; ++v) red[0][v] = red[1][v] = 0.0;
     const int t0 = il.a_cta[blockIdx.x], t1 = il.a_cta[blockIdx.x + 1];
-    if (t0 < t1) {
-        const IlTile first = il.a_tiles[t0];
-        if (first.staged) stage_tile_async(first, il.a_ptr, il.a_idx, il.a_val, st[0]);
-    }
     for (int ti = t0; ti < t1; ++ti) {
         const IlTile t = il.a_tiles[ti];
-        copy_async_wait();
-        __syncthreads();
-        if (ti + 1 < t1) {
-            const IlTile nt = il.a_tiles[ti + 1];
-            if (nt.staged) stage_tile_async(nt, il.a_ptr, il.a_idx, il.a_val, st[(ti + 1 - t0) & 1]);
+        if (t.staged) {
+            stage_row_tile(il, t, st);
+            copy_async_wait();
+            __syncthreads();
+            dual_tile_segmented<kFam>(x, t, st, red);
+        } else {
+            dual_line_global<kFam>(x, t, red);
         }
-        if (t.staged) dual_tile<kDualU<T, V>, true, kFam>(x, t, st[(ti - t0) & 1], red);
-        else dual_tile<1, false, kFam>(x, t, st[0], red);
         __syncthreads();
     }
     double cta[2];

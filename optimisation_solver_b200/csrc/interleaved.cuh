@@ -38,6 +38,12 @@ namespace pdlpgpu {
 // memory (staged = 0).
 constexpr int kIlTileLines = 64;
 constexpr int kIlTileEntries = 1536;
+// The dual splits each row into segments of at most kIlSegEntries entries; a
+// warp gathers one segment's entries at once and a row adds its segments'
+// partial sums in order. A staged row tile holds at most kIlTileSegs
+// segments.
+constexpr int kIlSegEntries = 8;
+constexpr int kIlTileSegs = 32;
 
 struct IlTile {
     int64_t e0;        // first entry
@@ -91,6 +97,10 @@ struct Interleaved {
     // [col_ctas + 1]; CTA line ranges are balanced by entries)
     const IlTile* a_tiles;
     const IlTile* at_tiles;
+    // row segments: row i's segments are a_lseg[i] .. a_lseg[i + 1] - 1;
+    // segment q starts at entry a_segstart[q]
+    const int32_t* a_lseg;      // [m + 1]
+    const int64_t* a_segstart;  // [segments + 1]
     const int32_t* a_cta;
     const int32_t* at_cta;
     // Per-instance sums, two levels: every CTA writes its partial, the last
