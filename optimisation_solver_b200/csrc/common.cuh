@@ -97,7 +97,7 @@ struct alignas(64) InstanceCtl {
     int32_t have_avg_at_check;
     int32_t stall_checks;
     int32_t il_sync;        // interleaved layout: the iterate was copied out for a check
-    int32_t pad0;
+    int32_t to_fp64;        // mixed: the check moves the instance to the FP64 stage
     // --- counters
     int64_t iteration;       // main phase: committed iterations (state.iteration)
     int64_t step_trials;     // main phase trials

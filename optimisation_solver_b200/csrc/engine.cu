@@ -84,6 +84,7 @@ Engine::~Engine() {
         if (e) cudaEventDestroy(e);
     for (void* q : extra_) cudaFree(q);
     if (graph_) cudaGraphExecDestroy(graph_);
+    if (graph64_) cudaGraphExecDestroy(graph64_);
     if (arena_) cudaFree(arena_);
     if (h_active_) cudaFreeHost(h_active_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -309,7 +310,7 @@ bool Engine::prepare(const SolveSpec& spec) {
     plan.add(g_.part_check, kCheckSlots * static_cast<int64_t>(a_ctas_.size() + at_ctas_.size()));
     plan.add(g_.count_dual, count_);
     plan.add(g_.count_check, count_);
-    plan.add(d_active_, 1);
+    plan.add(d_active_, 2);
     auto plan_work = [&](auto& w, int64_t Rn, int64_t Nn) {
         for (int k = 0; k < 2; ++k) {
             plan.add(w.X[k], Nn);
@@ -324,7 +325,7 @@ bool Engine::prepare(const SolveSpec& spec) {
     arena_bytes_ = plan.total();
     if (!check(cudaMalloc(&arena_, arena_bytes_), "cudaMalloc")) return false;
     plan.assign(arena_);
-    if (!check(cudaMallocHost(&h_active_, sizeof(int32_t)), "cudaMallocHost")) return false;
+    if (!check(cudaMallocHost(&h_active_, 2 * sizeof(int32_t)), "cudaMallocHost")) return false;
     if (!check(cudaMemsetAsync(arena_, 0, arena_bytes_, stream_), "cudaMemset")) return false;
 
     // --- host staging and upload ------------------------------------------
@@ -384,6 +385,7 @@ bool Engine::prepare(const SolveSpec& spec) {
         g_.num_vec = static_cast<int32_t>(vec_.size());
         g_.info = d_info;
         g_.shared_matrix = spec.shared_matrix ? 1 : 0;
+        g_.mixed = mixed_ ? 1 : 0;
         g_.warm_x = nullptr;
         g_.warm_y = nullptr;
         // A^T-side data bases, slice indices and line bases in info_ and in the
@@ -667,10 +669,13 @@ void Engine::enqueue_check_stage(bool il_sync) {
     launch_check_spmv(g_, dopt_, V, stream_);
     if (mixed_) launch_check_apply<float>(g_, w32_, dopt_, stream_);
     launch_check_apply<double>(g_, w64_, dopt_, stream_);
+    // Mixed: instances the check moves to the FP64 stage take their last
+    // FP32 restart point as the FP64 iterate (its A x is refreshed next).
+    if (mixed_) launch_switch_fp64(g_, w32_, w64_, stream_);
     if (mixed_) launch_refresh<float>(g_, w32_, dopt_, V, stream_);
     launch_refresh<double>(g_, w64_, dopt_, V, stream_);
     if (sync) il_move_iterates(false, kIlSynced, nullptr);
-    cudaMemsetAsync(d_active_, 0, sizeof(int32_t), stream_);
+    cudaMemsetAsync(d_active_, 0, 2 * sizeof(int32_t), stream_);
     launch_finalize(g_, count_, d_active_, stream_);
     launches_ += check_stage_launches(il_sync);
 }
@@ -691,10 +696,11 @@ int Engine::timed_position(int k, int slots) const {
     return -1;
 }
 
-void Engine::enqueue_chunk(int slots) {
-    // A mixed solve iterates in FP32; the FP64 trial kernels are captured only
-    // for the FP64 stage graph. Four slots' kernels are bracketed by timing
-    // events.
+void Engine::enqueue_chunk(int slots, bool fp64_stage) {
+    // A mixed solve iterates in FP32; while some instance is in its FP64
+    // stage, each slot also launches the per-instance FP64 trial kernels
+    // (each kernel runs only the instances of its precision). Four slots'
+    // kernels are bracketed by timing events.
     record_timing(0);
     for (int k = 0; k < slots; ++k) {
         const int p = timed_position(k, slots);
@@ -705,7 +711,7 @@ void Engine::enqueue_chunk(int slots) {
             if (p >= 0) record_timing(4 + 3 * p);
             if (mixed_) launch_il_dual<float>(il32_, g_.ctl, dopt_, 0, k, stream_);
             else launch_il_dual<double>(il64_, g_.ctl, dopt_, 0, k, stream_);
-        } else if (mixed_ && !fp64_graph_) {
+        } else if (mixed_) {
             launch_primal<float>(g_, w32_, dopt_, tuning_.vector_width, stream_);
             if (p >= 0) record_timing(4 + 3 * p);
             launch_dual<float>(g_, w32_, dopt_, tuning_.vector_width, stream_);
@@ -716,6 +722,11 @@ void Engine::enqueue_chunk(int slots) {
         }
         launches_ += 2;
         if (p >= 0) record_timing(5 + 3 * p);
+        if (mixed_ && fp64_stage) {
+            launch_primal<double>(g_, w64_, dopt_, tuning_.vector_width, stream_);
+            launch_dual<double>(g_, w64_, dopt_, tuning_.vector_width, stream_);
+            launches_ += 2;
+        }
     }
     record_timing(1);
     enqueue_check_stage(true);
@@ -775,32 +786,43 @@ void Engine::loop_timing(double* out) const {
     }
 }
 
-bool Engine::build_graph(int slots) {
+bool Engine::build_graph(int slots, bool fp64_stage) {
     cudaGraph_t graph = nullptr;
     if (!check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture"))
         return false;
     const int64_t before = launches_;
-    enqueue_chunk(slots);
+    enqueue_chunk(slots, fp64_stage);
     launches_ = before;
     if (!check(cudaStreamEndCapture(stream_, &graph), "end capture")) return false;
-    const bool ok = check(cudaGraphInstantiate(&graph_, graph, 0), "graph instantiate");
+    const bool ok = check(cudaGraphInstantiate(fp64_stage ? &graph64_ : &graph_, graph, 0), "graph instantiate");
     cudaGraphDestroy(graph);
     graph_slots_ = slots;
     graph_family_ = il_family_;
     return ok;
 }
 
+bool Engine::launch_chunk(int slots) {
+    // h_active_[1]: instances in the FP64 stage at the last poll.
+    const bool fp64 = mixed_ && h_active_[1] > 0;
+    const int per_chunk = 2 * slots * (fp64 ? 2 : 1) + check_stage_launches(true);
+    if (spec_.ext.disable_graphs) {
+        enqueue_chunk(slots, fp64);
+        return check(cudaGetLastError(), "chunk launch");
+    }
+    cudaGraphExec_t& g = fp64 ? graph64_ : graph_;
+    if (g == nullptr && !build_graph(slots, fp64)) return false;
+    launches_ += per_chunk;
+    return check(cudaGraphLaunch(g, stream_), "graph launch");
+}
+
 bool Engine::run() {
     if (!setup_ok_ || count_ == 0) return setup_ok_;
     const pdlpgpu_options& o = spec_.opt;
-    if (!check(cudaMemcpyAsync(h_active_, d_active_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "poll"))
+    if (!check(cudaMemcpyAsync(h_active_, d_active_, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "poll"))
         return false;
     if (!check(cudaStreamSynchronize(stream_), "setup")) return false;
     const int slack = spec_.ext.chunk_slack > 0 ? spec_.ext.chunk_slack : 4;
     const int slots = chunk_slots();
-    const bool graphs = spec_.ext.disable_graphs == 0;
-    if (*h_active_ != 0 && graphs && graph_ == nullptr && !build_graph(slots)) return false;
-    const int per_chunk = 2 * slots + check_stage_launches(true);
     const int64_t trials_bound =
         (std::max<int64_t>(o.iteration_limit, 0) + std::max(o.polishing_iterations, 0) + 2) *
         std::max(o.maximum_step_trials, 1);
@@ -816,14 +838,9 @@ bool Engine::run() {
             error_ = "device loop exceeded its chunk bound";
             break;
         }
-        if (graphs) {
-            if (!check(cudaGraphLaunch(graph_, stream_), "graph launch")) break;
-            launches_ += per_chunk;
-        } else {
-            enqueue_chunk(slots);
-        }
+        if (!launch_chunk(slots)) break;
         ++chunks;
-        cudaMemcpyAsync(h_active_, d_active_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
+        cudaMemcpyAsync(h_active_, d_active_, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
         if (!check(cudaStreamSynchronize(stream_), "iteration loop")) break;
         timing_collect(slots);
     }
@@ -1387,14 +1404,16 @@ bool Engine::time_kernels(int reps, double* out) {
 // Streams
 // ---------------------------------------------------------------------------
 bool Engine::ensure_graph() {
-    if (graph_ != nullptr && il_ && graph_family_ != il_family_) {
+    if (il_ && graph_family_ != il_family_) {
         // The captured interleaved kernels address the family vectors of the
         // load they were captured with.
-        cudaGraphExecDestroy(graph_);
-        graph_ = nullptr;
+        for (cudaGraphExec_t* g : {&graph_, &graph64_}) {
+            if (*g != nullptr) cudaGraphExecDestroy(*g);
+            *g = nullptr;
+        }
     }
     if (graph_ != nullptr || spec_.ext.disable_graphs) return true;
-    return build_graph(chunk_slots());
+    return build_graph(chunk_slots(), false);
 }
 
 bool Engine::session_stream(bool on_device, int64_t N, const double* const in[5], const double* wx,
@@ -1460,7 +1479,6 @@ bool Engine::session_stream(bool on_device, int64_t N, const double* const in[5]
     int64_t next = 0;
     const int slack = spec_.ext.chunk_slack > 0 ? spec_.ext.chunk_slack : 4;
     const int slots = graph_slots_ > 0 ? graph_slots_ : chunk_slots();
-    const int per_chunk = 2 * slots + check_stage_launches(true);
     launches_ = 0;
 
     auto upload_slots = [&]() {
@@ -1564,6 +1582,7 @@ bool Engine::session_stream(bool on_device, int64_t N, const double* const in[5]
     while (ok) {
         launch_slot_done(g_, B, d_done_, stream_);
         ok = check(cudaMemcpyAsync(done.data(), d_done_, done.size() * 4, cudaMemcpyDeviceToHost, stream_), "poll") &&
+             check(cudaMemcpyAsync(h_active_, d_active_, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "poll") &&
              check(cudaStreamSynchronize(stream_), "poll");
         if (!ok) break;
         if (chunks > 0) timing_collect(slots);
@@ -1577,12 +1596,7 @@ bool Engine::session_stream(bool on_device, int64_t N, const double* const in[5]
             ok = false;
             break;
         }
-        if (graph_) {
-            ok = check(cudaGraphLaunch(graph_, stream_), "graph launch");
-            launches_ += per_chunk;
-        } else {
-            enqueue_chunk(slots);
-        }
+        ok = launch_chunk(slots);
     }
     cudaEventRecord(e1, stream_);
     cudaEventSynchronize(e1);

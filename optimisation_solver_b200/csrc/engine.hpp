@@ -86,7 +86,10 @@ public:
 private:
     template <class T> void enqueue_trial(const Work<T>& w);
     template <class T> void enqueue_check(const Work<T>& w);
-    void enqueue_chunk(int slots);
+    void enqueue_chunk(int slots, bool fp64_stage);
+    // One chunk: the captured graph with or without the FP64 trial kernels,
+    // as the last poll's count of FP64-stage instances asks.
+    bool launch_chunk(int slots);
     // The check stage; with `il_sync` the iterates of the instances at a
     // check are moved out of the interleaved layout first and back after.
     void enqueue_check_stage(bool il_sync = false);
@@ -103,7 +106,7 @@ private:
     void il_move_iterates(bool to_planar, int select, const int32_t* mask);
     void il_move_statics(int select, const int32_t* mask);
     bool check(cudaError_t e, const char* what);
-    bool build_graph(int slots);
+    bool build_graph(int slots, bool fp64_stage);
     bool ensure_graph();
     bool power_iteration();
     bool setup_kernels();
@@ -114,7 +117,8 @@ private:
     int device_ = 0;
     int sms_ = 148;
     cudaStream_t stream_ = nullptr;
-    cudaGraphExec_t graph_ = nullptr;
+    cudaGraphExec_t graph_ = nullptr;     // chunk with the working precision's trial kernels
+    cudaGraphExec_t graph64_ = nullptr;   // mixed: plus the FP64-stage trial kernels
     int graph_slots_ = 0;
     char* arena_ = nullptr;
     size_t arena_bytes_ = 0;
@@ -147,12 +151,11 @@ private:
     double* at_s64_ = nullptr;
     float* a_s32_ = nullptr;
     float* at_s32_ = nullptr;
-    int32_t* d_active_ = nullptr;
-    int32_t* h_active_ = nullptr;     // pinned
+    int32_t* d_active_ = nullptr;     // [2]: unfinished instances, those in the FP64 stage
+    int32_t* h_active_ = nullptr;     // pinned copy
     double device_seconds_ = 0.0;
     int64_t launches_ = 0;
     bool ran_ = false;
-    bool fp64_graph_ = false;           // capturing the FP64-stage chunk of a mixed solve
     bool setup_ok_ = false;
     // session state
     std::vector<void*> extra_;              // device allocations beyond the arena

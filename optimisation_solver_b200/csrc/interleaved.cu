@@ -817,7 +817,7 @@ __global__ void __launch_bounds__(256) k_il_move(IlMove<T> mv) {
             switch (mv.select) {
                 case kIlAll: s = 1; break;
                 case kIlMasked: s = mv.mask[b] != 0; break;
-                case kIlAtCheck: s = c.stage == kStageCheck; break;
+                case kIlAtCheck: s = c.stage == kStageCheck && precision_matches<T>(c); break;
                 default: s = c.il_sync != 0; break;
             }
             p = c.parity;

@@ -610,6 +610,23 @@ __device__ __noinline__ void check_decide(const DeviceOptions& o, InstanceCtl& c
         c.since_restart = 0;
         ++c.restart_count;
     }
+    if (o.mixed && !c.fp64_stage) {
+        // Mixed precision: FP32 iterations go on while the best KKT score
+        // keeps falling; after fp32_stall_checks checks without a 10% drop the
+        // instance continues in FP64 from its last FP32 restart point (the
+        // restart point this check may just have set), with a fresh average.
+        if (!(c.best_kkt_at_stall > 0.0) || c.best_kkt < 0.9 * c.best_kkt_at_stall) {
+            c.best_kkt_at_stall = c.best_kkt;
+            c.stall_checks = 0;
+        } else if (++c.stall_checks >= o.fp32_stall_checks) {
+            c.to_fp64 = 1;
+            c.need_refresh = 1;
+            c.avg_weight = 0.0;
+            c.since_restart = 0;
+            c.prev_candidate = INFINITY;
+            c.stall_checks = 0;
+        }
+    }
     loop_top_main(c, o, n_cols);
 }
 
@@ -799,7 +816,8 @@ template <class T, int V>
 __global__ void __launch_bounds__(kThreads) k_refresh(Global g, Work<T> w) {
     const CtaWork cw = g.a.ctas[blockIdx.x];
     const InstanceCtl& c = g.ctl[cw.instance];
-    if (!c.need_refresh || !precision_matches<T>(c)) return;
+    // An instance moving to the FP64 stage gets its FP64 product here.
+    if (!c.need_refresh || !(precision_matches<T>(c) || (sizeof(T) == 8 && c.to_fp64))) return;
     const InstanceInfo inf = g.info[cw.instance];
     const int p = c.parity;
     const T* __restrict__ x = w.X[p] + inf.col_off;
@@ -818,11 +836,21 @@ __global__ void __launch_bounds__(kThreads) k_refresh(Global g, Work<T> w) {
     }
 }
 
+// Clears the per-check flags, completes a move to the FP64 stage, and counts
+// the unfinished instances (active[0]) and those among them in the FP64
+// stage of a mixed solve (active[1]).
 __global__ void k_finalize(Global g, int32_t count, int32_t* active) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= count) return;
     InstanceCtl& c = g.ctl[b];
-    if (c.phase != kPhaseDone && active != nullptr) atomicAdd(active, 1);
+    if (c.to_fp64) {
+        c.fp64_stage = 1;
+        c.to_fp64 = 0;
+    }
+    if (c.phase != kPhaseDone && active != nullptr) {
+        atomicAdd(active, 1);
+        if (c.fp64_stage && g.mixed) atomicAdd(active + 1, 1);
+    }
     if (c.stage == kStageCheck && c.check_kind == kCheckTransition) c.stage = kStageTrial;
     c.best_src = 0;
     c.restart_src = 0;
@@ -836,7 +864,7 @@ __global__ void k_finalize(Global g, int32_t count, int32_t* active) {
 __global__ void k_switch_fp64(Global g, Work<float> w32, Work<double> w64) {
     const VecWork vw = g.vec[blockIdx.x];
     const InstanceCtl& c = g.ctl[vw.instance];
-    if (!c.to_polish || !c.fp64_stage) return;   // reused flag: set with fp64_stage on the switch
+    if (!c.to_fp64) return;
     const InstanceInfo inf = g.info[vw.instance];
     const int p = c.parity;
     if (!vw.is_row) {

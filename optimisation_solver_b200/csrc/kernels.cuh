@@ -83,6 +83,8 @@ struct Global {
     // 1: timing mode -- every instance runs its trial kernels, no decision is
     // taken and no state changes (the trial buffers are scratch).
     int32_t measure;
+    // 1: mixed-precision solve (FP32 iterations, FP64 stage on stall)
+    int32_t mixed;
     // Streams: when set, setup kernels act only on slots with slot_mask[b] != 0.
     const int32_t* slot_mask;
 };
@@ -103,6 +105,8 @@ void launch_check_apply(const Global& g, const Work<T>& w, const DeviceOptions& 
 template <class T>
 void launch_refresh(const Global& g, const Work<T>& w, const DeviceOptions& o, int vw,
                     cudaStream_t s);
+// active[0]: unfinished instances; active[1]: those in the FP64 stage of a
+// mixed solve (both must be zeroed first).
 void launch_finalize(const Global& g, int32_t count, int32_t* active, cudaStream_t s);
 void launch_switch_fp64(const Global& g, const Work<float>& w32, const Work<double>& w64,
                         cudaStream_t s);
