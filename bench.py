@@ -63,6 +63,10 @@ def parse_args():
                    help="skip the cold-start, plain-GPU and large-LP side measurements")
     p.add_argument("--profile", action="store_true",
                    help="a short cold stream only (for ncu captures of the trial kernels)")
+    p.add_argument("--workload", choices=["flow", "large", "stress", "uneven"], default="flow",
+                   help="flow: the headline (config 4); large, stress, uneven: configs 1, 3 and 2, "
+                        "each reported on its own line")
+    p.add_argument("--count", type=int, default=1024, help="uneven: instances in the batch")
     return p.parse_args()
 
 
@@ -195,6 +199,10 @@ def main():
 
     if args.impl == "reference":
         return reference_arm(args, world, rank, graph, config)
+    if args.workload != "flow":
+        if rank == 0:
+            print(json.dumps(side_workload(args)))
+        return
 
     import torch
     import torch.distributed as dist
@@ -355,6 +363,94 @@ def main():
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+
+
+def _kernel_roofline(tk):
+    peak, kind = peaks()
+    out = {}
+    for name, ms, nbytes in (("primal", tk["primal_ms"], tk["primal_bytes"]),
+                             ("dual", tk["dual_ms"], tk["dual_bytes"])):
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        out[name] = {"launch_us": round(ms * 1e3, 1), "algorithmic_bytes": nbytes,
+                     "gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+    out["peak_gbs"] = peak
+    out["peak_source"] = kind
+    return out
+
+
+def _planted_instance(args):
+    from optimisation_solver_b200 import generators as g
+    i, m = args
+    rng = np.random.default_rng(40_000 + i)
+    deg = rng.integers(4, 13, size=2 * int(m))
+    return g.planted_lp(int(m), 2 * int(m), seed=i, degrees=deg)
+
+
+def side_workload(args):
+    """Configs 1-3, one JSON line each: solve time, PDHG iterations/s, the
+    trial kernels' algorithmic GB/s (CUDA events, every instance active) and
+    each result's objective error against the planted FP64 optimum."""
+    import torch
+    from optimisation_solver_b200 import generators as g
+    from optimisation_solver_b200.lp import PdlpOptions
+    from optimisation_solver_b200.pdlp import PdlpSolver
+    torch.cuda.set_device(0)
+    opts = PdlpOptions().with_tolerance(args.tol)
+    line = {"workload": args.workload, "tolerance": args.tol, "data": "synthetic (seeded generators)"}
+    if args.workload in ("large", "stress"):
+        p = g.large_lp(0) if args.workload == "large" else g.stress_lp(0)
+        line["config"] = {"rows": p.lp.num_rows, "cols": p.lp.num_cols, "nnz": int(p.lp.nnz)}
+        line["metric"] = "PDHG iterations/s, trial-kernel GB/s, objective error vs planted optimum"
+        from optimisation_solver_b200.autotune import tune
+        for prec in ("fp64", "mixed"):
+            tuned = tune([p.lp], opts, precision=prec, reps=5)
+            solver = PdlpSolver(prec, **tuned["params"])
+            tk = solver.time_kernels_batch([p.lp], opts, reps=20)
+            r = solver.solve(p.lp, opts)
+            line[prec] = {"status": str(r.status), "iterations": r.iterations,
+                          "precision": r.precision, "fp64_iterations": r.fp64_iterations,
+                          "device_seconds": round(r.device_seconds, 3),
+                          "iterations_per_s": round(r.iterations / max(r.device_seconds, 1e-9), 1),
+                          "objective_rel_error": abs(r.primal_objective - p.objective) / (1 + abs(p.objective)),
+                          "primal_residual": r.primal_residual, "dual_residual": r.dual_residual,
+                          "relative_gap": r.relative_gap, "kernels": _kernel_roofline(tk),
+                          "tuned": {"params": tuned["params"], "trial_ms": round(tuned["trial_ms"], 4),
+                                    "default_trial_ms": round(tuned["default_trial_ms"], 4)}}
+        return line
+    # uneven: config 2, `count` LPs of uneven sizes in one batched solve
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    sizes = g.uneven_batch_sizes(args.count)
+    t0 = time.perf_counter()
+    with ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1),
+                             mp_context=mp.get_context("spawn")) as ex:
+        lps = list(ex.map(_planted_instance, list(enumerate(sizes)), chunksize=8))
+    gen = time.perf_counter() - t0
+    nnz = int(sum(q.lp.nnz for q in lps))
+    line["config"] = {"instances": args.count, "sum_rows": int(sizes.sum()), "sum_cols": int(2 * sizes.sum()),
+                      "nnz": nnz, "generation_seconds": round(gen, 1)}
+    line["metric"] = "LPs solved/s at 1e-4 rel. KKT, one batched solve (config 2)"
+    from optimisation_solver_b200.autotune import tune
+    tuned = tune([q.lp for q in lps], opts, precision=args.precision, reps=3,
+                 grid={"lane_elements": (8, 32), "vector_width": (1, 4), "cta_slots": (0,)})
+    solver = PdlpSolver(args.precision, **tuned["params"])
+    tk = solver.time_kernels_batch([q.lp for q in lps], opts, reps=10)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = solver.solve_batch([q.lp for q in lps], opts)
+    wall = time.perf_counter() - t0
+    its = np.array([r.iterations for r in res])
+    err = np.array([abs(r.primal_objective - q.objective) / (1 + abs(q.objective)) for r, q in zip(res, lps)])
+    ok = np.array([r.status == 0 for r in res])
+    line.update({"value": round(args.count / wall, 2), "unit": "LPs/s", "wall_seconds": round(wall, 2),
+                 "device_seconds": round(max(r.device_seconds for r in res), 2),
+                 "optimal_fraction": float(ok.mean()), "mean_iterations": float(its.mean()),
+                 "max_iterations": int(its.max()),
+                 "objective_rel_error_max": float(err[ok].max()) if ok.any() else None,
+                 "kernels": _kernel_roofline(tk), "precision": args.precision,
+                 "tuned": {"params": tuned["params"], "trial_ms": round(tuned["trial_ms"], 4),
+                           "default_trial_ms": round(tuned["default_trial_ms"], 4)}})
+    return line
 
 
 def extras(args, session, graph, sup, cost, inputs, value, iters, solve):

@@ -121,7 +121,7 @@ typedef struct pdlpgpu_ext_options {
     int32_t vector_width;          /* SpMV tuning: 1, 2 or 4 elements per lane load (0 = autotune) */
     int32_t chunk_slack;           /* extra trial slots per captured check interval (0 = 4) */
     int32_t fp32_stall_checks;     /* mixed: checks without progress before the FP64 stage (0 = 8) */
-    int32_t fp32_switch_factor;    /* mixed: FP64 stage once KKT <= factor * tol fails to improve (0 = 1) */
+    int32_t fp32_switch_factor;    /* mixed: stalls count once the best KKT <= factor * tol (0 = 1000) */
     int32_t disable_graphs;        /* 1: launch kernels directly instead of CUDA graphs */
     int32_t cta_slots;             /* SpMV tuning: matrix slots per CTA (0 = autotune) */
     int32_t layout;                /* sessions: PDLPGPU_LAYOUT_* */
@@ -189,6 +189,16 @@ int32_t pdlpgpu_solve_ex(const pdlpgpu_lp* lp, const pdlpgpu_options* options,
 int32_t pdlpgpu_solve_batch(const pdlpgpu_lp* const* lps, int32_t count,
                             const pdlpgpu_options* options, const pdlpgpu_ext_options* ext,
                             const pdlpgpu_warmstart* const* warm, pdlpgpu_result** results);
+
+/* Times the two PDHG trial kernels of a batch of LPs (as pdlpgpu_solve_batch
+ * lays them out) with CUDA events, `reps` launches each, every instance
+ * active, after the setup; no solve. out[6] = {primal ms per launch, dual ms
+ * per launch, primal algorithmic bytes per launch, dual algorithmic bytes per
+ * launch, padded slots of the A^T side, padded slots of the A side}. No
+ * counterpart in the reference. Returns 0, or -1 with pdlpgpu_last_error(). */
+int32_t pdlpgpu_batch_time_kernels(const pdlpgpu_lp* const* lps, int32_t count,
+                                   const pdlpgpu_options* options, const pdlpgpu_ext_options* ext,
+                                   int32_t reps, double* out);
 
 void pdlpgpu_result_free(pdlpgpu_result* result);
 

@@ -154,6 +154,27 @@ int32_t pdlpgpu_solve_batch(const pdlpgpu_lp* const* lps, int32_t count,
     }
 }
 
+int32_t pdlpgpu_batch_time_kernels(const pdlpgpu_lp* const* lps, int32_t count,
+                                   const pdlpgpu_options* options, const pdlpgpu_ext_options* ext,
+                                   int32_t reps, double* out) {
+    if (lps == nullptr || out == nullptr || count <= 0 || reps <= 0) return -1;
+    try {
+        pdlpgpu::SolveSpec spec;
+        spec.lps.assign(lps, lps + count);
+        spec.opt = opt_or_default(options);
+        spec.ext = ext_or_default(ext);
+        pdlpgpu::Engine engine(spec.ext.device);
+        if (!engine.setup(spec) || !engine.time_kernels(reps, out)) {
+            set_error(engine.error());
+            return -1;
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return -1;
+    }
+}
+
 void pdlpgpu_result_free(pdlpgpu_result* r) {
     if (r == nullptr) return;
     std::free(r->primal);

@@ -170,6 +170,7 @@ struct DeviceOptions {
     int32_t max_restart;
     int32_t mixed;             // iterations in FP32 first
     int32_t fp32_stall_checks;
+    double fp32_switch_kkt;    // mixed: stalls count once the best KKT score is at most this
     double primal_tol, dual_tol, gap_tol;
     double min_step_scale;
     double w_min, w_max, smoothing;

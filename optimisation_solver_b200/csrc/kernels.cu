@@ -95,9 +95,10 @@ __device__ __forceinline__ void line_sums(int64_t base, int steps, const LanePos
                                           int len, const int32_t* __restrict__ idx,
                                           const TV* __restrict__ val, TA (&acc)[NQ], F fetch) {
     constexpr int kDepth = V >= 4 ? 1 : 4 / V;   // about four entries in flight per lane
-    for (int s0 = 0; s0 < steps; s0 += kDepth * V) {
-        int32_t id[kDepth][V];
-        TV v[kDepth][V];
+    constexpr int kStep = kDepth * V;
+    // Software pipeline: the index and value loads of the next group are in
+    // flight while the current group's gathers are.
+    auto load = [&](int s0, int32_t (&id)[kDepth][V], TV (&v)[kDepth][V]) {
 #pragma unroll
         for (int u = 0; u < kDepth; ++u) {
             const int s = s0 + u * V;
@@ -113,6 +114,14 @@ __device__ __forceinline__ void line_sums(int64_t base, int steps, const LanePos
                 }
             }
         }
+    };
+    int32_t id[kDepth][V];
+    TV v[kDepth][V];
+    load(0, id, v);
+    for (int s0 = 0; s0 < steps; s0 += kStep) {
+        int32_t nid[kDepth][V];
+        TV nv[kDepth][V];
+        load(s0 + kStep, nid, nv);
 #pragma unroll
         for (int u = 0; u < kDepth; ++u) {
 #pragma unroll
@@ -121,6 +130,13 @@ __device__ __forceinline__ void line_sums(int64_t base, int steps, const LanePos
                 if (k < len) fetch(acc, static_cast<TA>(v[u][q]), id[u][q]);
             }
         }
+#pragma unroll
+        for (int u = 0; u < kDepth; ++u)
+#pragma unroll
+            for (int q = 0; q < V; ++q) {
+                id[u][q] = nid[u][q];
+                v[u][q] = nv[u][q];
+            }
     }
     for (int o = (1 << lp.glog) >> 1; o > 0; o >>= 1) {
 #pragma unroll
@@ -195,7 +211,7 @@ template <> __device__ __forceinline__ const float* matrix_values<float>(const S
 // Primal half (pdhg_kernel.cpp:47-104)
 // ---------------------------------------------------------------------------
 template <class T, int V>
-__global__ void __launch_bounds__(kThreads, 6) k_primal(Global g, Work<T> w) {
+__global__ void __launch_bounds__(kThreads, 4) k_primal(Global g, Work<T> w) {
     const CtaWork cw = g.at.ctas[blockIdx.x];
     const InstanceCtl& c = g.ctl[cw.instance];
     if (!g.measure && !trial_active<T>(c)) return;
@@ -257,7 +273,7 @@ __global__ void __launch_bounds__(kThreads, 6) k_primal(Global g, Work<T> w) {
 // Dual half (pdhg_kernel.cpp:109-187) and the trial decision
 // ---------------------------------------------------------------------------
 template <class T, int V>
-__global__ void __launch_bounds__(kThreads, 6) k_dual(Global g, Work<T> w, DeviceOptions o) {
+__global__ void __launch_bounds__(kThreads, 4) k_dual(Global g, Work<T> w, DeviceOptions o) {
     const CtaWork cw = g.a.ctas[blockIdx.x];
     InstanceCtl& c = g.ctl[cw.instance];
     if (!g.measure && !trial_active<T>(c)) return;
@@ -612,10 +628,12 @@ __device__ __noinline__ void check_decide(const DeviceOptions& o, InstanceCtl& c
     }
     if (o.mixed && !c.fp64_stage) {
         // Mixed precision: FP32 iterations go on while the best KKT score
-        // keeps falling; after fp32_stall_checks checks without a 10% drop the
+        // keeps falling or is still far (above fp32_switch_kkt) from the
+        // tolerance; after fp32_stall_checks checks without a 10% drop the
         // instance continues in FP64 from its last FP32 restart point (the
         // restart point this check may just have set), with a fresh average.
-        if (!(c.best_kkt_at_stall > 0.0) || c.best_kkt < 0.9 * c.best_kkt_at_stall) {
+        if (!(c.best_kkt_at_stall > 0.0) || c.best_kkt < 0.9 * c.best_kkt_at_stall ||
+            !(c.best_kkt <= o.fp32_switch_kkt)) {
             c.best_kkt_at_stall = c.best_kkt;
             c.stall_checks = 0;
         } else if (++c.stall_checks >= o.fp32_stall_checks) {

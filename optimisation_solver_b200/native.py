@@ -115,6 +115,8 @@ SIGNATURES = {
                                [_i32p, _i64p, _dp]),
     "pdlpgpu_session_time_kernels": (C.c_int32, [C.c_void_p, C.c_int32, _dp]),
     "pdlpgpu_session_loop_timing": (C.c_int32, [C.c_void_p, _dp]),
+    "pdlpgpu_batch_time_kernels": (C.c_int32, [C.POINTER(C.POINTER(Lp)), C.c_int32, C.POINTER(Options),
+                                               C.POINTER(ExtOptions), C.c_int32, _dp]),
     "pdlpgpu_mlp_create": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
                                        C.c_int32, C.POINTER(C.c_void_p)]),
     "pdlpgpu_mlp_destroy": (None, [C.c_void_p]),

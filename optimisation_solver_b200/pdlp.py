@@ -110,6 +110,21 @@ class PdlpSolver:
                 L.pdlpgpu_result_free(outs[i])
 
 
+    def time_kernels_batch(self, problems, options: PdlpOptions | None = None, reps: int = 10) -> dict:
+        """The two trial kernels of a batch laid out as solve_batch lays it out,
+        timed with every instance active (no solve)."""
+        hs = [native.LpHandle(p) for p in problems]
+        arr = (C.POINTER(native.Lp) * len(hs))(*[C.pointer(h.struct) for h in hs])
+        o = native.options_struct(options or PdlpOptions())
+        e = self._ext()
+        out = np.zeros(6)
+        rc = native.lib().pdlpgpu_batch_time_kernels(arr, len(hs), C.byref(o), C.byref(e), reps,
+                                                     native.ptr(out))
+        _check(rc, "batch_time_kernels")
+        return dict(primal_ms=out[0], dual_ms=out[1], primal_bytes=out[2], dual_bytes=out[3],
+                    at_padding=out[4], a_padding=out[5])
+
+
 # ---------------------------------------------------------------------------
 # Components (include/pdlpgpu_components.h)
 # ---------------------------------------------------------------------------
