@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <thread>
 
 namespace pdlpgpu {
@@ -75,6 +76,20 @@ void normalisers(const pdlpgpu_lp& lp, double& pnorm, double& dnorm) {
 template <class T>
 void fill_value(std::vector<T>& v, size_t n, T x) { v.assign(n, x); }
 
+// f(k) for k in [0, count), spread over the host's hardware threads.
+template <class F>
+void parallel_for(int count, F f) {
+    const int threads = std::min<int>(count, std::max(1u, std::thread::hardware_concurrency()));
+    if (threads <= 1) {
+        for (int k = 0; k < count; ++k) f(k);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t)
+        pool.emplace_back([&, t] { for (int k = t; k < count; k += threads) f(k); });
+    for (auto& th : pool) th.join();
+}
+
 }  // namespace
 
 Engine::Engine(int device) : device_(device) {}
@@ -123,7 +138,7 @@ bool Engine::prepare(const SolveSpec& spec) {
     std::vector<HostCsr> csr(static_cast<size_t>(spec.shared_matrix ? 1 : nspec));
     std::string shared_error;
     if (spec.shared_matrix && nspec > 0) shared_error = canonicalize(*spec.lps[0], csr[0]);
-    for (int i = 0; i < nspec; ++i) {
+    parallel_for(nspec, [&](int i) {
         const pdlpgpu_lp& lp = *spec.lps[i];
         std::string err;
         if (spec.shared_matrix) {
@@ -135,7 +150,7 @@ bool Engine::prepare(const SolveSpec& spec) {
         }
         if (err.empty()) err = validate_vectors(lp);
         invalid_[i] = err;
-    }
+    });
     const bool bad_options = o.iteration_limit < 0 || o.termination_check_frequency <= 0 ||
                              o.primal_tolerance < 0.0 || o.dual_tolerance < 0.0 ||
                              o.gap_tolerance < 0.0 || o.initial_step_safety <= 0.0 ||
@@ -336,23 +351,33 @@ bool Engine::prepare(const SolveSpec& spec) {
     {
         std::vector<SliceDesc> slices;
         slices.reserve(static_cast<size_t>(a_slices_ + at_slices_));
-        std::vector<int32_t> idx;
-        std::vector<double> val;
-        idx.reserve(static_cast<size_t>(slots));
-        val.reserve(static_cast<size_t>(slots));
-        for (int k = 0; k < nlayouts; ++k) {
+        for (int k = 0; k < nlayouts; ++k)
             slices.insert(slices.end(), layouts_[k].a.slices.begin(), layouts_[k].a.slices.end());
-            idx.insert(idx.end(), layouts_[k].a.idx.begin(), layouts_[k].a.idx.end());
-            val.insert(val.end(), layouts_[k].a.val.begin(), layouts_[k].a.val.end());
-        }
-        for (int k = 0; k < nlayouts; ++k) {
+        for (int k = 0; k < nlayouts; ++k)
             slices.insert(slices.end(), layouts_[k].at.slices.begin(), layouts_[k].at.slices.end());
-            idx.insert(idx.end(), layouts_[k].at.idx.begin(), layouts_[k].at.idx.end());
-            val.insert(val.end(), layouts_[k].at.val.begin(), layouts_[k].at.val.end());
+        // Slot data of every layout, A side then A^T side, copied in parallel
+        // into one staging buffer each (left uninitialised: every slot is
+        // written).
+        std::vector<int64_t> a_at(static_cast<size_t>(nlayouts) + 1, 0), at_at(static_cast<size_t>(nlayouts) + 1, 0);
+        for (int k = 0; k < nlayouts; ++k) {
+            a_at[static_cast<size_t>(k) + 1] = a_at[static_cast<size_t>(k)] + layouts_[k].a.slots();
+            at_at[static_cast<size_t>(k) + 1] = at_at[static_cast<size_t>(k)] + layouts_[k].at.slots();
         }
+        std::unique_ptr<int32_t[]> idx(new int32_t[static_cast<size_t>(std::max<int64_t>(slots, 1))]);
+        std::unique_ptr<double[]> val(new double[static_cast<size_t>(std::max<int64_t>(slots, 1))]);
+        parallel_for(nlayouts, [&](int k) {
+            const SideLayout& A = layouts_[k].a;
+            const SideLayout& T = layouts_[k].at;
+            std::copy(A.idx.begin(), A.idx.end(), idx.get() + a_at[static_cast<size_t>(k)]);
+            std::copy(A.val.begin(), A.val.end(), val.get() + a_at[static_cast<size_t>(k)]);
+            std::copy(T.idx.begin(), T.idx.end(), idx.get() + a_slots_ + at_at[static_cast<size_t>(k)]);
+            std::copy(T.val.begin(), T.val.end(), val.get() + a_slots_ + at_at[static_cast<size_t>(k)]);
+        });
         if (!up(d_slices, slices.data(), slices.size() * sizeof(SliceDesc))) return false;
-        if (!up(d_idx, idx.data(), idx.size() * sizeof(int32_t))) return false;
-        if (!up(d_val, val.data(), val.size() * sizeof(double))) return false;
+        if (!up(d_idx, idx.get(), static_cast<size_t>(slots) * sizeof(int32_t))) return false;
+        if (!up(d_val, val.get(), static_cast<size_t>(slots) * sizeof(double))) return false;
+        // The staging buffers go out of scope here: the pageable copies above
+        // have read them before cudaMemcpyAsync returned.
         std::vector<int32_t> len;
         len.reserve(static_cast<size_t>(lens));
         for (int k = 0; k < nlayouts; ++k) len.insert(len.end(), layouts_[k].a.line_len.begin(), layouts_[k].a.line_len.end());
