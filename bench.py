@@ -146,9 +146,10 @@ class ClockSampler:
 
 def workload(batch: int, steps: int, rank: int, graph):
     """Per-step (supply, cost) of fresh instances, seeded per rank and step
-    (disjoint from the training seeds)."""
+    (disjoint across ranks and from the training seeds)."""
     from optimisation_solver_b200 import generators as g
-    return [g.flow_parameters(graph, batch, seed=100_000 * (rank + 1) + k) for k in range(steps)]
+    from optimisation_solver_b200.sharding import rank_seeds
+    return [g.flow_parameters(graph, batch, seed=sd) for sd in rank_seeds(rank, steps)]
 
 
 def cpu_solve_sample(lib_kind: str, graph, supply, cost, tol: float, threads: int):
@@ -199,9 +200,22 @@ def main():
 
     if args.impl == "reference":
         return reference_arm(args, world, rank, graph, config)
-    if args.workload != "flow":
+    if args.workload in ("large", "stress"):
+        # One LP: replicas only, so rank 0 measures it.
         if rank == 0:
-            print(json.dumps(side_workload(args)))
+            print(json.dumps(side_workload(args, 0, 1, 0)))
+        return
+    if args.workload == "uneven":
+        # Instances split across ranks, balanced by nonzeros.
+        import torch.distributed as dist
+        if world > 1:
+            dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        line = side_workload(args, rank, world, local_rank)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(line))
         return
 
     import torch
@@ -282,11 +296,8 @@ def main():
     loop = session.loop_timing()
     if world > 1:
         dist.barrier()
-    elapsed = start.elapsed_time(end) / 1e3
-    t = torch.tensor([elapsed], device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_max = float(t.item())
+    from optimisation_solver_b200.sharding import max_over_ranks
+    elapsed_max = max_over_ranks(start.elapsed_time(end) / 1e3, dev)
     value = world * K * B / elapsed_max
     optimal = res["optimal"]
     iters = res["iterations"]
@@ -311,10 +322,7 @@ def main():
     out_yh.copy_(py, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
-    t = torch.tensor([e0.elapsed_time(e1) / 1e3], device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * K * B / float(t.item())
+    e2e_value = world * K * B / max_over_ranks(e0.elapsed_time(e1) / 1e3, dev)
 
     # Roofline of the dominant trial kernel, live durations from the events
     # captured in the timed loop.
@@ -386,15 +394,19 @@ def _planted_instance(args):
     return g.planted_lp(int(m), 2 * int(m), seed=i, degrees=deg)
 
 
-def side_workload(args):
+def side_workload(args, rank: int, world: int, local_rank: int):
     """Configs 1-3, one JSON line each: solve time, PDHG iterations/s, the
     trial kernels' algorithmic GB/s (CUDA events, every instance active) and
-    each result's objective error against the planted FP64 optimum."""
+    each result's objective error against the planted FP64 optimum. Config 2
+    splits its instances across the ranks (nonzero-balanced, strong
+    scaling)."""
     import torch
     from optimisation_solver_b200 import generators as g
     from optimisation_solver_b200.lp import PdlpOptions
     from optimisation_solver_b200.pdlp import PdlpSolver
-    torch.cuda.set_device(0)
+    from optimisation_solver_b200.sharding import balanced_shards, max_over_ranks, sum_over_ranks
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
     opts = PdlpOptions().with_tolerance(args.tol)
     line = {"workload": args.workload, "tolerance": args.tol, "data": "synthetic (seeded generators)"}
     if args.workload in ("large", "stress"):
@@ -421,14 +433,16 @@ def side_workload(args):
     import multiprocessing as mp
     from concurrent.futures import ProcessPoolExecutor
     sizes = g.uneven_batch_sizes(args.count)
+    mine = balanced_shards(sizes * 16, world)[rank]   # about 16 nonzeros per row
     t0 = time.perf_counter()
     with ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1),
                              mp_context=mp.get_context("spawn")) as ex:
-        lps = list(ex.map(_planted_instance, list(enumerate(sizes)), chunksize=8))
+        lps = list(ex.map(_planted_instance, [(int(i), sizes[i]) for i in mine], chunksize=8))
     gen = time.perf_counter() - t0
-    nnz = int(sum(q.lp.nnz for q in lps))
+    nnz = int(sum_over_ranks(sum(q.lp.nnz for q in lps), dev))
     line["config"] = {"instances": args.count, "sum_rows": int(sizes.sum()), "sum_cols": int(2 * sizes.sum()),
-                      "nnz": nnz, "generation_seconds": round(gen, 1)}
+                      "nnz": nnz, "generation_seconds": round(gen, 1), "n_gpus": world,
+                      "scaling": "strong" if world > 1 else None}
     line["metric"] = "LPs solved/s at 1e-4 rel. KKT, one batched solve (config 2)"
     from optimisation_solver_b200.autotune import tune
     tuned = tune([q.lp for q in lps], opts, precision=args.precision, reps=3,
@@ -436,15 +450,19 @@ def side_workload(args):
     solver = PdlpSolver(args.precision, **tuned["params"])
     tk = solver.time_kernels_batch([q.lp for q in lps], opts, reps=10)
     torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
     t0 = time.perf_counter()
     res = solver.solve_batch([q.lp for q in lps], opts)
-    wall = time.perf_counter() - t0
+    wall = max_over_ranks(time.perf_counter() - t0, dev)
     its = np.array([r.iterations for r in res])
     err = np.array([abs(r.primal_objective - q.objective) / (1 + abs(q.objective)) for r, q in zip(res, lps)])
     ok = np.array([r.status == 0 for r in res])
     line.update({"value": round(args.count / wall, 2), "unit": "LPs/s", "wall_seconds": round(wall, 2),
-                 "device_seconds": round(max(r.device_seconds for r in res), 2),
-                 "optimal_fraction": float(ok.mean()), "mean_iterations": float(its.mean()),
+                 "device_seconds": round(max_over_ranks(max(r.device_seconds for r in res), dev), 2),
+                 "optimal_fraction": sum_over_ranks(float(ok.sum()), dev) / args.count,
+                 "mean_iterations": float(its.mean()),
                  "max_iterations": int(its.max()),
                  "objective_rel_error_max": float(err[ok].max()) if ok.any() else None,
                  "kernels": _kernel_roofline(tk), "precision": args.precision,
