@@ -121,7 +121,7 @@ typedef struct pdlpgpu_ext_options {
     int32_t vector_width;          /* SpMV tuning: 1, 2 or 4 elements per lane load (0 = autotune) */
     int32_t chunk_slack;           /* extra trial slots per captured check interval (0 = 4) */
     int32_t fp32_stall_checks;     /* mixed: checks without progress before the FP64 stage (0 = 8) */
-    int32_t fp32_switch_factor;    /* mixed: stalls count once the best KKT <= factor * tol (0 = 1000) */
+    int32_t fp32_switch_factor;    /* mixed: stalls count once the best KKT <= min(factor * tol, 1e-5) (0 = 1000) */
     int32_t disable_graphs;        /* 1: launch kernels directly instead of CUDA graphs */
     int32_t cta_slots;             /* SpMV tuning: matrix slots per CTA (0 = autotune) */
     int32_t layout;                /* sessions: PDLPGPU_LAYOUT_* */

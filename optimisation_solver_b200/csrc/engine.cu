@@ -494,11 +494,12 @@ bool Engine::prepare(const SolveSpec& spec) {
     dopt_.max_restart = o.maximum_restart_iterations;
     dopt_.mixed = mixed_ ? 1 : 0;
     dopt_.fp32_stall_checks = spec.ext.fp32_stall_checks > 0 ? spec.ext.fp32_stall_checks : 8;
-    // FP32 stalls far above the tolerance are the method's, not the
-    // precision's: the FP64 stage is considered only within a factor of the
-    // largest tolerance.
-    dopt_.fp32_switch_kkt = (spec.ext.fp32_switch_factor > 0 ? spec.ext.fp32_switch_factor : 1000) *
-                            std::max({spec.opt.primal_tolerance, spec.opt.dual_tolerance, spec.opt.gap_tolerance});
+    // FP32 stalls far above the tolerance, or above the relative KKT level
+    // FP32 iterates reach without difficulty (1e-5), are the method's, not
+    // the precision's: the FP64 stage is considered only below both.
+    dopt_.fp32_switch_kkt = std::min(
+        1e-5, (spec.ext.fp32_switch_factor > 0 ? spec.ext.fp32_switch_factor : 1000) *
+                  std::max({spec.opt.primal_tolerance, spec.opt.dual_tolerance, spec.opt.gap_tolerance}));
     dopt_.primal_tol = o.primal_tolerance;
     dopt_.dual_tol = o.dual_tolerance;
     dopt_.gap_tol = o.gap_tolerance;

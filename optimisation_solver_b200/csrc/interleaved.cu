@@ -17,6 +17,8 @@
 #include "control.cuh"
 #include "interleaved.cuh"
 
+#include <utility>
+
 namespace pdlpgpu {
 namespace {
 
@@ -38,6 +40,15 @@ __device__ __forceinline__ bool arrive_last_cta(int32_t* counter, int expected) 
     if (last) __threadfence();
     return last != 0;
 }
+
+// Programmatic dependent launch: the trial kernels are launched so that the
+// next one may start while this one finishes. A kernel waits for its
+// predecessor (wait) before it touches anything the predecessor writes --
+// the control blocks, the iterates, the partial sums -- and lets its own
+// successor start (trigger) only after that wait, so a successor never runs
+// ahead of a still-running decision two kernels back.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // V consecutive elements (one 4/8/16-byte access).
 template <class T, int V>
@@ -518,8 +529,19 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_primal(Interleaved<T> il, 
     PrimalCtx<T, V> x;
     x.il = &il;
     x.col0 = static_cast<int64_t>(group) * G + lane * V;
+    // The matrix does not change: its first tile is staged before the wait.
+    const int t0 = il.at_cta[blockIdx.x], t1 = il.at_cta[blockIdx.x + 1];
+    if (t0 < t1) {
+        const IlTile first = il.at_tiles[t0];
+        if (first.staged) stage_tile_async(first, il.at_ptr, il.at_idx, il.at_val, st[0]);
+    }
+    pdl_wait();
+    pdl_trigger();
     x.ls = lane_state<T, V>(il, ctl, static_cast<int>(x.col0), measure, R, true, hot);
-    if (!__syncthreads_or(x.ls.active != 0)) return;
+    if (!__syncthreads_or(x.ls.active != 0)) {
+        copy_async_wait();
+        return;
+    }
     x.XR = il.X[R];
     x.XW_read = il.X[W];
     x.xr = il.X[R];
@@ -534,11 +556,6 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_primal(Interleaved<T> il, 
     double moved[1][V];
 #pragma unroll
     for (int v = 0; v < V; ++v) moved[0][v] = 0.0;
-    const int t0 = il.at_cta[blockIdx.x], t1 = il.at_cta[blockIdx.x + 1];
-    if (t0 < t1) {
-        const IlTile first = il.at_tiles[t0];
-        if (first.staged) stage_tile_async(first, il.at_ptr, il.at_idx, il.at_val, st[0]);
-    }
     for (int ti = t0; ti < t1; ++ti) {
         const IlTile t = il.at_tiles[ti];
         copy_async_wait();
@@ -729,8 +746,14 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_dual(Interleaved<T> il, In
     DualCtx<T, V> x;
     x.il = &il;
     x.col0 = static_cast<int64_t>(group) * G + lane * V;
+    // The control blocks were last written by the decision of the previous
+    // dual kernel, which is complete (see pdl_wait): read before the wait.
     x.ls = lane_state<T, V>(il, ctl, static_cast<int>(x.col0), measure, R, false, sm.hot);
     if (!__syncthreads_or(x.ls.active != 0)) return;
+    const int t0 = il.a_cta[blockIdx.x], t1 = il.a_cta[blockIdx.x + 1];
+    if (t0 < t1 && il.a_tiles[t0].staged) stage_row_tile(il, il.a_tiles[t0], st);
+    pdl_wait();
+    pdl_trigger();
     x.xt = il.X[W] + x.col0;
     x.YR = il.Y[R];
     x.YW = il.Y[W];
@@ -747,11 +770,10 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_dual(Interleaved<T> il, In
     double red[2][V];
 #pragma unroll
     for (int v = 0; v < V; ++v) red[0][v] = red[1][v] = 0.0;
-    const int t0 = il.a_cta[blockIdx.x], t1 = il.a_cta[blockIdx.x + 1];
     for (int ti = t0; ti < t1; ++ti) {
         const IlTile t = il.a_tiles[ti];
         if (t.staged) {
-            stage_row_tile(il, t, st);
+            if (ti != t0) stage_row_tile(il, t, st);
             copy_async_wait();
             __syncthreads();
             dual_tile_segmented<kFam>(x, t, st, red);
@@ -925,6 +947,23 @@ int il_blocks_per_sm(int vl, bool dual) {
 
 namespace {
 
+// A trial kernel launched with programmatic stream serialization (see
+// pdl_wait): it may start while the previous kernel in the stream finishes.
+template <class... P, class... A>
+void launch_pdl(void (*kernel)(P...), dim3 grid, cudaStream_t s, A&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(kIlThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
+
 constexpr int32_t kXBounds = (1 << kIlXl) | (1 << kIlXu);
 constexpr int32_t kRBounds = (1 << kIlRl) | (1 << kIlRu);
 
@@ -932,9 +971,9 @@ template <class T, int V>
 void primal_v(const Interleaved<T>& il, InstanceCtl* ctl, int measure, int slot, cudaStream_t s) {
     const dim3 grid(il.col_ctas, il.groups);
     if ((il.family & kXBounds) == kXBounds)
-        k_il_primal<T, V, true><<<grid, kIlThreads, 0, s>>>(il, ctl, measure, slot);
+        launch_pdl(k_il_primal<T, V, true>, grid, s, il, ctl, measure, slot);
     else
-        k_il_primal<T, V, false><<<grid, kIlThreads, 0, s>>>(il, ctl, measure, slot);
+        launch_pdl(k_il_primal<T, V, false>, grid, s, il, ctl, measure, slot);
 }
 
 template <class T, int V>
@@ -942,9 +981,9 @@ void dual_v(const Interleaved<T>& il, InstanceCtl* ctl, const DeviceOptions& o, 
             cudaStream_t s) {
     const dim3 grid(il.row_ctas, il.groups);
     if ((il.family & kRBounds) == kRBounds)
-        k_il_dual<T, V, true><<<grid, kIlThreads, 0, s>>>(il, ctl, o, measure, slot);
+        launch_pdl(k_il_dual<T, V, true>, grid, s, il, ctl, o, measure, slot);
     else
-        k_il_dual<T, V, false><<<grid, kIlThreads, 0, s>>>(il, ctl, o, measure, slot);
+        launch_pdl(k_il_dual<T, V, false>, grid, s, il, ctl, o, measure, slot);
 }
 
 }  // namespace
