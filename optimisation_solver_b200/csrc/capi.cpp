@@ -339,12 +339,11 @@ int32_t pdlpgpu_layout_stats(const pdlpgpu_lp* lp, const pdlpgpu_ext_options* ex
             set_error(err);
             return -1;
         }
-        const pdlpgpu::HostCsr at = pdlpgpu::transpose(a);
-        pdlpgpu::Tuning t = pdlpgpu::choose_tuning(a, at, ext && ext->precision == PDLPGPU_PRECISION_MIXED);
+        pdlpgpu::Tuning t = pdlpgpu::choose_tuning(a, ext && ext->precision == PDLPGPU_PRECISION_MIXED);
         if (ext && ext->lane_elements > 0) t.lane_elements = ext->lane_elements;
         if (ext && (ext->vector_width == 1 || ext->vector_width == 2 || ext->vector_width == 4))
             t.vector_width = ext->vector_width;
-        const pdlpgpu::MatrixLayout L = pdlpgpu::build_layout(a, at, t);
+        const pdlpgpu::MatrixLayout L = pdlpgpu::build_layout(a, t);
         stats[0] = static_cast<int64_t>(L.a.slices.size());
         stats[1] = L.a.slots();
         stats[2] = L.a.entries;
@@ -369,12 +368,11 @@ int32_t pdlpgpu_layout_multiply(const pdlpgpu_lp* lp, const pdlpgpu_ext_options*
             set_error(err);
             return -1;
         }
-        const pdlpgpu::HostCsr at = pdlpgpu::transpose(a);
-        pdlpgpu::Tuning t = pdlpgpu::choose_tuning(a, at, false);
+        pdlpgpu::Tuning t = pdlpgpu::choose_tuning(a, false);
         if (ext && ext->lane_elements > 0) t.lane_elements = ext->lane_elements;
         if (ext && (ext->vector_width == 1 || ext->vector_width == 2 || ext->vector_width == 4))
             t.vector_width = ext->vector_width;
-        const pdlpgpu::MatrixLayout L = pdlpgpu::build_layout(a, at, t);
+        const pdlpgpu::MatrixLayout L = pdlpgpu::build_layout(a, t);
         const int V = t.vector_width;
         std::vector<double> xin(static_cast<size_t>(L.n));
         for (int32_t c = 0; c < L.n; ++c) xin[c] = x[L.col_perm[c]];

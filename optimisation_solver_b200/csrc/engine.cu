@@ -6,10 +6,12 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <numeric>
 #include <thread>
 
 namespace pdlpgpu {
@@ -90,9 +92,140 @@ void parallel_for(int count, F f) {
     for (auto& th : pool) th.join();
 }
 
+// f(k) for k in [0, count), each k to the next free host thread.
+template <class F>
+void parallel_dynamic(int count, F f) {
+    const int threads = std::min<int>(count, std::max(1u, std::thread::hardware_concurrency()));
+    if (threads <= 1) {
+        for (int k = 0; k < count; ++k) f(k);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t)
+        pool.emplace_back([&] {
+            for (int k = next++; k < count; k = next++) f(k);
+        });
+    for (auto& th : pool) th.join();
+}
+
 }  // namespace
 
 Engine::Engine(int device) : device_(device) {}
+
+void Engine::mark(const char* phase) {
+    static const bool on = [] {
+        const char* v = std::getenv("PDLPGPU_TRACE");
+        return v != nullptr && v[0] == '1';
+    }();
+    if (!on) return;
+    trace_.emplace_back(phase, std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count());
+}
+
+namespace {
+constexpr size_t kPinnedChunk = size_t(64) << 20;   // bytes per staging buffer
+constexpr size_t kPinnedDirect = size_t(4) << 20;   // smaller uploads go as they are
+constexpr size_t kCopyJob = size_t(2) << 20;        // host memcpy piece per thread
+}  // namespace
+
+bool Engine::ensure_pinned() {
+    for (int b = 0; b < 2; ++b) {
+        if (pinned_[b] == nullptr &&
+            !check(cudaHostAlloc(reinterpret_cast<void**>(&pinned_[b]), kPinnedChunk, cudaHostAllocDefault), "cudaHostAlloc"))
+            return false;
+        if (pinned_done_[b] == nullptr &&
+            !check(cudaEventCreateWithFlags(&pinned_done_[b], cudaEventDisableTiming), "cudaEventCreate"))
+            return false;
+    }
+    return true;
+}
+
+// The reverse path: the DMA of the next chunk into one pinned buffer runs
+// while all host threads copy the previous chunk out of the other.
+bool Engine::download(void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return true;
+    if (bytes < kPinnedDirect)
+        return check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream_), "download") &&
+               check(cudaStreamSynchronize(stream_), "download");
+    if (!ensure_pinned()) return false;
+    const size_t chunks = (bytes + kPinnedChunk - 1) / kPinnedChunk;
+    auto enqueue = [&](size_t c) {
+        const size_t off = c * kPinnedChunk, n = std::min(kPinnedChunk, bytes - off);
+        return check(cudaMemcpyAsync(pinned_[c & 1], static_cast<const char*>(src) + off, n, cudaMemcpyDeviceToHost, stream_), "download") &&
+               check(cudaEventRecord(pinned_done_[c & 1], stream_), "download");
+    };
+    if (!enqueue(0)) return false;
+    for (size_t c = 0; c < chunks; ++c) {
+        if (c + 1 < chunks && !enqueue(c + 1)) return false;
+        if (!check(cudaEventSynchronize(pinned_done_[c & 1]), "download")) return false;
+        const size_t off = c * kPinnedChunk, n = std::min(kPinnedChunk, bytes - off);
+        const int jobs = static_cast<int>((n + kCopyJob - 1) / kCopyJob);
+        const char* from = pinned_[c & 1];
+        char* to = static_cast<char*>(dst) + off;
+        parallel_for(jobs, [&](int j) {
+            const size_t a = static_cast<size_t>(j) * kCopyJob;
+            std::memcpy(to + a, from + a, std::min(kCopyJob, n - a));
+        });
+    }
+    return true;
+}
+
+// A copy from pageable memory is staged by the driver through its own small
+// pinned buffers, one thread, and returns only when it is done: for the
+// gigabytes of a large batch's matrices that runs at a fraction of the host
+// link. Large uploads here go through two 64 MiB pinned buffers instead: all
+// host threads fill one while the other's DMA is in flight.
+bool Engine::upload(void* dst, const std::vector<HostPiece>& pieces) {
+    size_t total = 0;
+    for (const HostPiece& q : pieces) total += q.bytes;
+    if (total == 0) return true;
+    char* out = static_cast<char*>(dst);
+    if (total < kPinnedDirect) {
+        for (const HostPiece& q : pieces) {
+            if (q.bytes && !check(cudaMemcpyAsync(out, q.src, q.bytes, cudaMemcpyHostToDevice, stream_), "upload"))
+                return false;
+            out += q.bytes;
+        }
+        return true;
+    }
+    if (!ensure_pinned()) return false;
+    struct Job {
+        size_t at;          // offset in the staging buffer
+        const char* src;
+        size_t bytes;
+    };
+    std::vector<Job> jobs;
+    size_t piece = 0, in_piece = 0;   // read position
+    for (int chunk = 0; piece < pieces.size(); ++chunk) {
+        const int b = chunk & 1;
+        // Jobs of this chunk: up to kPinnedChunk bytes of the pieces, cut
+        // into at most kCopyJob bytes each.
+        jobs.clear();
+        size_t fill = 0;
+        while (fill < kPinnedChunk && piece < pieces.size()) {
+            const HostPiece& q = pieces[piece];
+            const size_t n = std::min({q.bytes - in_piece, kPinnedChunk - fill, kCopyJob});
+            if (n > 0) jobs.push_back({fill, static_cast<const char*>(q.src) + in_piece, n});
+            fill += n;
+            in_piece += n;
+            if (in_piece == q.bytes) {
+                ++piece;
+                in_piece = 0;
+            }
+        }
+        if (fill == 0) break;
+        // The buffer's previous copy must have finished before it is refilled.
+        if (!check(cudaEventSynchronize(pinned_done_[b]), "upload")) return false;
+        char* stage = pinned_[b];
+        parallel_for(static_cast<int>(jobs.size()),
+                     [&](int j) { std::memcpy(stage + jobs[j].at, jobs[j].src, jobs[j].bytes); });
+        if (!check(cudaMemcpyAsync(out, stage, fill, cudaMemcpyHostToDevice, stream_), "upload") ||
+            !check(cudaEventRecord(pinned_done_[b], stream_), "upload"))
+            return false;
+        out += fill;
+    }
+    return true;
+}
 
 Engine::~Engine() {
     for (cudaEvent_t e : tev_)
@@ -102,6 +235,10 @@ Engine::~Engine() {
     if (graph64_) cudaGraphExecDestroy(graph64_);
     if (arena_) cudaFree(arena_);
     if (h_active_) cudaFreeHost(h_active_);
+    for (int b = 0; b < 2; ++b) {
+        if (pinned_done_[b]) cudaEventDestroy(pinned_done_[b]);
+        if (pinned_[b]) cudaFreeHost(pinned_[b]);
+    }
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -164,6 +301,7 @@ bool Engine::prepare(const SolveSpec& spec) {
         setup_ok_ = true;
         return true;
     }
+    mark("validate");
 
     // --- device and tuning ------------------------------------------------
     if (!check(cudaSetDevice(device_), "cudaSetDevice")) return false;
@@ -175,7 +313,6 @@ bool Engine::prepare(const SolveSpec& spec) {
         if (e == nullptr && !check(cudaEventCreate(&e), "cudaEventCreate")) return false;
 
     // Layouts: one per device instance, or one shared.
-    std::vector<HostCsr> csrT;
     std::vector<int> spec_of(static_cast<size_t>(count_));
     for (int i = 0; i < nspec; ++i) if (device_of_[i] >= 0) spec_of[device_of_[i]] = i;
     const int nlayouts = spec.shared_matrix ? 1 : count_;
@@ -205,23 +342,20 @@ bool Engine::prepare(const SolveSpec& spec) {
     }
     layouts_.resize(static_cast<size_t>(nlayouts));
     {
-        auto build = [&](int k) {
+        // Largest matrices first, each to the next free thread.
+        std::vector<int> order(static_cast<size_t>(nlayouts));
+        std::iota(order.begin(), order.end(), 0);
+        auto nnz_of = [&](int k) { return csr[spec.shared_matrix ? 0 : spec_of[k]].nnz(); };
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return nnz_of(x) > nnz_of(y); });
+        parallel_dynamic(nlayouts, [&](int q) {
+            const int k = order[static_cast<size_t>(q)];
             const HostCsr& a = csr[spec.shared_matrix ? 0 : spec_of[k]];
-            const HostCsr at = transpose(a);
-            layouts_[k] = build_layout(a, at, tuning_);
-        };
-        const int threads = std::min<int>(nlayouts, std::max(1u, std::thread::hardware_concurrency()));
-        if (threads <= 1) {
-            for (int k = 0; k < nlayouts; ++k) build(k);
-        } else {
-            std::vector<std::thread> pool;
-            for (int t = 0; t < threads; ++t)
-                pool.emplace_back([&, t] { for (int k = t; k < nlayouts; k += threads) build(k); });
-            for (auto& th : pool) th.join();
-        }
+            layouts_[k] = build_layout(a, tuning_);
+        });
     }
     if (!csr.empty()) csr0_ = std::move(csr[spec.shared_matrix ? 0 : spec_of[0]]);
     csr.clear();
+    mark("layouts");
 
     // --- spaces, slices and CTA maps --------------------------------------
     info_.resize(static_cast<size_t>(count_));
@@ -342,12 +476,10 @@ bool Engine::prepare(const SolveSpec& spec) {
     plan.assign(arena_);
     if (!check(cudaMallocHost(&h_active_, 2 * sizeof(int32_t)), "cudaMallocHost")) return false;
     if (!check(cudaMemsetAsync(arena_, 0, arena_bytes_, stream_), "cudaMemset")) return false;
+    mark("maps and arena");
 
     // --- host staging and upload ------------------------------------------
-    auto up = [&](void* dst, const void* src, size_t bytes) {
-        if (bytes == 0) return true;
-        return check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_), "upload");
-    };
+    auto up = [&](void* dst, const void* src, size_t bytes) { return upload(dst, src, bytes); };
     {
         std::vector<SliceDesc> slices;
         slices.reserve(static_cast<size_t>(a_slices_ + at_slices_));
@@ -355,29 +487,17 @@ bool Engine::prepare(const SolveSpec& spec) {
             slices.insert(slices.end(), layouts_[k].a.slices.begin(), layouts_[k].a.slices.end());
         for (int k = 0; k < nlayouts; ++k)
             slices.insert(slices.end(), layouts_[k].at.slices.begin(), layouts_[k].at.slices.end());
-        // Slot data of every layout, A side then A^T side, copied in parallel
-        // into one staging buffer each (left uninitialised: every slot is
-        // written).
-        std::vector<int64_t> a_at(static_cast<size_t>(nlayouts) + 1, 0), at_at(static_cast<size_t>(nlayouts) + 1, 0);
-        for (int k = 0; k < nlayouts; ++k) {
-            a_at[static_cast<size_t>(k) + 1] = a_at[static_cast<size_t>(k)] + layouts_[k].a.slots();
-            at_at[static_cast<size_t>(k) + 1] = at_at[static_cast<size_t>(k)] + layouts_[k].at.slots();
-        }
-        std::unique_ptr<int32_t[]> idx(new int32_t[static_cast<size_t>(std::max<int64_t>(slots, 1))]);
-        std::unique_ptr<double[]> val(new double[static_cast<size_t>(std::max<int64_t>(slots, 1))]);
-        parallel_for(nlayouts, [&](int k) {
-            const SideLayout& A = layouts_[k].a;
-            const SideLayout& T = layouts_[k].at;
-            std::copy(A.idx.begin(), A.idx.end(), idx.get() + a_at[static_cast<size_t>(k)]);
-            std::copy(A.val.begin(), A.val.end(), val.get() + a_at[static_cast<size_t>(k)]);
-            std::copy(T.idx.begin(), T.idx.end(), idx.get() + a_slots_ + at_at[static_cast<size_t>(k)]);
-            std::copy(T.val.begin(), T.val.end(), val.get() + a_slots_ + at_at[static_cast<size_t>(k)]);
-        });
+        // Slot data of every layout, A side then A^T side, straight from the
+        // layouts (which outlive the copies).
+        std::vector<HostPiece> idx, val;
+        for (int side = 0; side < 2; ++side)
+            for (int k = 0; k < nlayouts; ++k) {
+                const SideLayout& S = side == 0 ? layouts_[k].a : layouts_[k].at;
+                idx.push_back({S.idx.data(), S.idx.size() * sizeof(int32_t)});
+                val.push_back({S.val.data(), S.val.size() * sizeof(double)});
+            }
         if (!up(d_slices, slices.data(), slices.size() * sizeof(SliceDesc))) return false;
-        if (!up(d_idx, idx.get(), static_cast<size_t>(slots) * sizeof(int32_t))) return false;
-        if (!up(d_val, val.get(), static_cast<size_t>(slots) * sizeof(double))) return false;
-        // The staging buffers go out of scope here: the pageable copies above
-        // have read them before cudaMemcpyAsync returned.
+        if (!upload(d_idx, idx) || !upload(d_val, val)) return false;
         std::vector<int32_t> len;
         len.reserve(static_cast<size_t>(lens));
         for (int k = 0; k < nlayouts; ++k) len.insert(len.end(), layouts_[k].a.line_len.begin(), layouts_[k].a.line_len.end());
@@ -416,31 +536,36 @@ bool Engine::prepare(const SolveSpec& spec) {
         // A^T-side data bases, slice indices and line bases in info_ and in the
         // CTA map are relative to the g_.at pointers.
     }
+    mark("matrix upload");
     {
         // Original-problem vectors in internal order.
-        std::vector<double> cvec(static_cast<size_t>(N)), xl(static_cast<size_t>(N)), xu(static_cast<size_t>(N));
-        std::vector<double> rl(static_cast<size_t>(R)), ru(static_cast<size_t>(R));
+        // Every element is written below (the instances tile both spaces).
+        std::unique_ptr<double[]> cvec(new double[static_cast<size_t>(std::max<int64_t>(N, 1))]);
+        std::unique_ptr<double[]> xl(new double[static_cast<size_t>(std::max<int64_t>(N, 1))]);
+        std::unique_ptr<double[]> xu(new double[static_cast<size_t>(std::max<int64_t>(N, 1))]);
+        std::unique_ptr<double[]> rl(new double[static_cast<size_t>(std::max<int64_t>(R, 1))]);
+        std::unique_ptr<double[]> ru(new double[static_cast<size_t>(std::max<int64_t>(R, 1))]);
         std::vector<double> wx, wy;
         if (any_warm) {
             wx.assign(static_cast<size_t>(N), std::nan(""));
             wy.assign(static_cast<size_t>(R), std::nan(""));
         }
-        std::vector<double> tmp;
-        for (int i = 0; i < nspec; ++i) {
+        parallel_for(nspec, [&](int i) {
             const int b = device_of_[i];
-            if (b < 0) continue;
+            if (b < 0) return;
+            std::vector<double> tmp;
             const pdlpgpu_lp& lp = *spec.lps[i];
             const InstanceInfo& inf = info_[b];
             to_internal_cols(lp.objective, tmp, b);
-            std::copy(tmp.begin(), tmp.end(), cvec.begin() + inf.col_off);
+            std::copy(tmp.begin(), tmp.end(), cvec.get() + inf.col_off);
             to_internal_cols(lp.var_lower, tmp, b);
-            std::copy(tmp.begin(), tmp.end(), xl.begin() + inf.col_off);
+            std::copy(tmp.begin(), tmp.end(), xl.get() + inf.col_off);
             to_internal_cols(lp.var_upper, tmp, b);
-            std::copy(tmp.begin(), tmp.end(), xu.begin() + inf.col_off);
+            std::copy(tmp.begin(), tmp.end(), xu.get() + inf.col_off);
             to_internal_rows(lp.row_lower, tmp, b);
-            std::copy(tmp.begin(), tmp.end(), rl.begin() + inf.row_off);
+            std::copy(tmp.begin(), tmp.end(), rl.get() + inf.row_off);
             to_internal_rows(lp.row_upper, tmp, b);
-            std::copy(tmp.begin(), tmp.end(), ru.begin() + inf.row_off);
+            std::copy(tmp.begin(), tmp.end(), ru.get() + inf.row_off);
             const pdlpgpu_warmstart* w = (i < static_cast<int>(spec.warm.size())) ? spec.warm[i] : nullptr;
             if (w && w->primal) {
                 to_internal_cols(w->primal, tmp, b);
@@ -450,12 +575,13 @@ bool Engine::prepare(const SolveSpec& spec) {
                 to_internal_rows(w->row_dual, tmp, b);
                 std::copy(tmp.begin(), tmp.end(), wy.begin() + inf.row_off);
             }
-        }
-        if (!up(const_cast<double*>(g_.c_orig), cvec.data(), cvec.size() * 8)) return false;
-        if (!up(const_cast<double*>(g_.xl_orig), xl.data(), xl.size() * 8)) return false;
-        if (!up(const_cast<double*>(g_.xu_orig), xu.data(), xu.size() * 8)) return false;
-        if (!up(const_cast<double*>(g_.rl_orig), rl.data(), rl.size() * 8)) return false;
-        if (!up(const_cast<double*>(g_.ru_orig), ru.data(), ru.size() * 8)) return false;
+        });
+        const size_t nb = static_cast<size_t>(N) * 8, rb = static_cast<size_t>(R) * 8;
+        if (!up(const_cast<double*>(g_.c_orig), cvec.get(), nb)) return false;
+        if (!up(const_cast<double*>(g_.xl_orig), xl.get(), nb)) return false;
+        if (!up(const_cast<double*>(g_.xu_orig), xu.get(), nb)) return false;
+        if (!up(const_cast<double*>(g_.rl_orig), rl.get(), rb)) return false;
+        if (!up(const_cast<double*>(g_.ru_orig), ru.get(), rb)) return false;
         if (any_warm) {
             // NaN marks "no warm value": k_setup_vectors falls back to the cold point.
             if (!up(warm_x, wx.data(), wx.size() * 8)) return false;
@@ -463,21 +589,15 @@ bool Engine::prepare(const SolveSpec& spec) {
             g_.warm_x = warm_x;
             g_.warm_y = warm_y;
         }
-        std::vector<double> ones(static_cast<size_t>(std::max(R, N)), 1.0);
-        if (!up(g_.rs, ones.data(), static_cast<size_t>(R) * 8)) return false;
-        if (!up(g_.cs, ones.data(), static_cast<size_t>(N) * 8)) return false;
-        // Preconditioner defaults (disabled preconditioning keeps these).
-        if (!up(w64_.tau, ones.data(), static_cast<size_t>(N) * 8)) return false;
-        if (!up(w64_.itau, ones.data(), static_cast<size_t>(N) * 8)) return false;
-        if (!up(w64_.sigma, ones.data(), static_cast<size_t>(R) * 8)) return false;
-        if (!up(w64_.isigma, ones.data(), static_cast<size_t>(R) * 8)) return false;
+        // Unit scales and the preconditioner defaults (disabled
+        // preconditioning keeps these).
+        for (double* p : {g_.rs, w64_.sigma, w64_.isigma}) launch_fill<double>(p, R, 1.0, stream_);
+        for (double* p : {g_.cs, w64_.tau, w64_.itau}) launch_fill<double>(p, N, 1.0, stream_);
         if (mixed_) {
-            std::vector<float> f1(static_cast<size_t>(std::max(R, N)), 1.0f);
-            if (!up(w32_.tau, f1.data(), static_cast<size_t>(N) * 4)) return false;
-            if (!up(w32_.itau, f1.data(), static_cast<size_t>(N) * 4)) return false;
-            if (!up(w32_.sigma, f1.data(), static_cast<size_t>(R) * 4)) return false;
-            if (!up(w32_.isigma, f1.data(), static_cast<size_t>(R) * 4)) return false;
+            for (float* p : {w32_.sigma, w32_.isigma}) launch_fill<float>(p, R, 1.0f, stream_);
+            for (float* p : {w32_.tau, w32_.itau}) launch_fill<float>(p, N, 1.0f, stream_);
         }
+        if (!check(cudaGetLastError(), "fill")) return false;
     }
 
     // --- options and per-instance control ---------------------------------
@@ -514,6 +634,7 @@ bool Engine::prepare(const SolveSpec& spec) {
     dopt_.infeasibility_tol = o.infeasibility_tolerance;
     dopt_.time_limit = o.time_limit_seconds;
     setup_ok_ = true;
+    mark("vector upload");
     return true;
 }
 
@@ -678,6 +799,7 @@ bool Engine::start() {
     if (mixed_) launch_refresh<float>(g_, w32_, dopt_, tuning_.vector_width, stream_);
     launch_refresh<double>(g_, w64_, dopt_, tuning_.vector_width, stream_);
     enqueue_check_stage();
+    mark("start");
     return check(cudaGetLastError(), "initial check");
 }
 
@@ -852,6 +974,7 @@ bool Engine::run() {
     if (!check(cudaMemcpyAsync(h_active_, d_active_, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "poll"))
         return false;
     if (!check(cudaStreamSynchronize(stream_), "setup")) return false;
+    mark("device setup");
     const int slack = spec_.ext.chunk_slack > 0 ? spec_.ext.chunk_slack : 4;
     const int slots = chunk_slots();
     const int64_t trials_bound =
@@ -883,28 +1006,34 @@ bool Engine::run() {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     ran_ = true;
+    mark("iterations");
     return error_.empty();
 }
 
 void Engine::results(std::vector<pdlpgpu_result*>& out) {
     const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
     std::vector<InstanceCtl> ctl(static_cast<size_t>(count_));
-    std::vector<double> bx, by, dr, pr;
+    // Best points always, rays only when some instance ends with one (no
+    // zero fill: every element read is downloaded).
+    std::unique_ptr<double[]> bx, by, dr, pr;
     bool have = false;
     if (count_ > 0 && stream_ != nullptr && arena_ != nullptr) {
-        bx.resize(static_cast<size_t>(cols_total_));
-        by.resize(static_cast<size_t>(rows_total_));
-        dr.resize(static_cast<size_t>(rows_total_));
-        pr.resize(static_cast<size_t>(cols_total_));
-        have = check(cudaMemcpyAsync(ctl.data(), g_.ctl, ctl.size() * sizeof(InstanceCtl), cudaMemcpyDeviceToHost, stream_), "download") &&
-               check(cudaMemcpyAsync(bx.data(), g_.best_x, bx.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") &&
-               check(cudaMemcpyAsync(by.data(), g_.best_y, by.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") &&
-               check(cudaMemcpyAsync(dr.data(), g_.dray, dr.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") &&
-               check(cudaMemcpyAsync(pr.data(), g_.pray, pr.size() * 8, cudaMemcpyDeviceToHost, stream_), "download") &&
-               check(cudaStreamSynchronize(stream_), "download");
+        const size_t R = static_cast<size_t>(rows_total_), N = static_cast<size_t>(cols_total_);
+        bx.reset(new double[std::max<size_t>(N, 1)]);
+        by.reset(new double[std::max<size_t>(R, 1)]);
+        have = download(ctl.data(), g_.ctl, ctl.size() * sizeof(InstanceCtl)) &&
+               download(bx.get(), g_.best_x, N * 8) && download(by.get(), g_.best_y, R * 8);
+        bool rays = false;
+        for (const InstanceCtl& c : ctl) rays = rays || c.ray_kind != 0;
+        mark("download");
+        if (have && rays) {
+            dr.reset(new double[std::max<size_t>(R, 1)]);
+            pr.reset(new double[std::max<size_t>(N, 1)]);
+            have = download(dr.get(), g_.dray, R * 8) && download(pr.get(), g_.pray, N * 8);
+        }
     }
-    out.clear();
-    for (size_t i = 0; i < spec_.lps.size(); ++i) {
+    out.assign(spec_.lps.size(), nullptr);
+    parallel_for(static_cast<int>(spec_.lps.size()), [&](int i) {
         const pdlpgpu_lp& lp = *spec_.lps[i];
         auto* r = static_cast<pdlpgpu_result*>(std::calloc(1, sizeof(pdlpgpu_result)));
         r->num_rows = lp.num_rows;
@@ -918,16 +1047,16 @@ void Engine::results(std::vector<pdlpgpu_result*>& out) {
         if (b < 0) {
             r->status = PDLPGPU_INVALID_PROBLEM;
             std::snprintf(r->status_message, sizeof(r->status_message), "%s", invalid_[i].c_str());
-            out.push_back(r);
-            continue;
+            out[i] = r;
+            return;
         }
         const InstanceCtl& c = ctl[static_cast<size_t>(b)];
         if (!have || c.phase != kPhaseDone || c.status < 0) {
             r->status = PDLPGPU_NUMERICAL_FAILURE;
             std::snprintf(r->status_message, sizeof(r->status_message), "%s",
                           error_.empty() ? "device loop did not complete" : error_.c_str());
-            out.push_back(r);
-            continue;
+            out[i] = r;
+            return;
         }
         const MatrixLayout& L = layouts_[spec_.shared_matrix ? 0 : b];
         const InstanceInfo& inf = info_[b];
@@ -935,15 +1064,15 @@ void Engine::results(std::vector<pdlpgpu_result*>& out) {
         std::snprintf(r->status_message, sizeof(r->status_message), "%s", message_text(c.message));
         r->primal = static_cast<double*>(std::malloc(sizeof(double) * std::max(1, lp.num_cols)));
         r->row_dual = static_cast<double*>(std::malloc(sizeof(double) * std::max(1, lp.num_rows)));
-        for (int32_t k = 0; k < inf.n; ++k) r->primal[L.col_perm[k]] = bx[inf.col_off + k];
-        for (int32_t k = 0; k < inf.m; ++k) r->row_dual[L.row_perm[k]] = by[inf.row_off + k];
-        if (c.status == PDLPGPU_INFEASIBLE && c.ray_kind == 1) {
+        for (int32_t k = 0; k < inf.n; ++k) r->primal[L.col_perm[k]] = bx[static_cast<size_t>(inf.col_off) + k];
+        for (int32_t k = 0; k < inf.m; ++k) r->row_dual[L.row_perm[k]] = by[static_cast<size_t>(inf.row_off) + k];
+        if (c.status == PDLPGPU_INFEASIBLE && c.ray_kind == 1 && dr) {
             r->dual_ray = static_cast<double*>(std::malloc(sizeof(double) * std::max(1, lp.num_rows)));
-            for (int32_t k = 0; k < inf.m; ++k) r->dual_ray[L.row_perm[k]] = dr[inf.row_off + k];
+            for (int32_t k = 0; k < inf.m; ++k) r->dual_ray[L.row_perm[k]] = dr[static_cast<size_t>(inf.row_off) + k];
         }
-        if (c.status == PDLPGPU_UNBOUNDED && c.ray_kind == 2) {
+        if (c.status == PDLPGPU_UNBOUNDED && c.ray_kind == 2 && pr) {
             r->primal_ray = static_cast<double*>(std::malloc(sizeof(double) * std::max(1, lp.num_cols)));
-            for (int32_t k = 0; k < inf.n; ++k) r->primal_ray[L.col_perm[k]] = pr[inf.col_off + k];
+            for (int32_t k = 0; k < inf.n; ++k) r->primal_ray[L.col_perm[k]] = pr[static_cast<size_t>(inf.col_off) + k];
         }
         r->primal_objective = c.best_pobj;
         r->dual_objective = c.best_dobj;
@@ -961,7 +1090,18 @@ void Engine::results(std::vector<pdlpgpu_result*>& out) {
         r->precision_used = mixed_ ? (c.fp64_stage ? 2 : 1) : 0;
         r->fp64_iterations = c.fp64_iterations;
         r->device_seconds = device_seconds_;
-        out.push_back(r);
+        out[i] = r;
+    });
+    mark("results");
+    if (!trace_.empty()) {
+        std::fprintf(stderr, "pdlpgpu:");
+        double prev = 0.0;
+        for (const auto& t : trace_) {
+            std::fprintf(stderr, " %s %.3f s;", t.first, t.second - prev);
+            prev = t.second;
+        }
+        std::fprintf(stderr, " total %.3f s\n", prev);
+        trace_.clear();
     }
 }
 

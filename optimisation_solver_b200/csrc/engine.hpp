@@ -98,7 +98,6 @@ private:
     // --- batch-interleaved layout (sessions)
     template <class T> bool il_build(Interleaved<T>& il, const Work<T>& w);
     void il_set_family(int32_t family);
-    void il_enqueue_trial(int slot, int measure);
     template <class T> IlMove<T> il_iterates(const Interleaved<T>& il, const Work<T>& w,
                                              bool to_planar, int select, const int32_t* mask) const;
     template <class T> IlMove<T> il_statics(const Interleaved<T>& il, const Work<T>& w, int select,
@@ -106,6 +105,21 @@ private:
     void il_move_iterates(bool to_planar, int select, const int32_t* mask);
     void il_move_statics(int select, const int32_t* mask);
     bool check(cudaError_t e, const char* what);
+    // Host-to-device copy of consecutive host pieces into dst (stream order).
+    struct HostPiece {
+        const void* src;
+        size_t bytes;
+    };
+    bool upload(void* dst, const std::vector<HostPiece>& pieces);
+    bool upload(void* dst, const void* src, size_t bytes) { return upload(dst, {{src, bytes}}); }
+    // Device-to-host copy, complete on return.
+    bool download(void* dst, const void* src, size_t bytes);
+    bool ensure_pinned();
+    // Host phases of a solve, with PDLPGPU_TRACE=1 in the environment: the
+    // seconds since the solve began at the end of each phase, printed to
+    // stderr once the results are assembled.
+    void mark(const char* phase);
+    std::vector<std::pair<const char*, double>> trace_;
     bool build_graph(int slots, bool fp64_stage);
     bool ensure_graph();
     bool power_iteration();
@@ -153,6 +167,9 @@ private:
     float* at_s32_ = nullptr;
     int32_t* d_active_ = nullptr;     // [2]: unfinished instances, those in the FP64 stage
     int32_t* h_active_ = nullptr;     // pinned copy
+    // two pinned staging buffers of large uploads and their last copies
+    char* pinned_[2] = {nullptr, nullptr};
+    cudaEvent_t pinned_done_[2] = {nullptr, nullptr};
     double device_seconds_ = 0.0;
     int64_t launches_ = 0;
     bool ran_ = false;

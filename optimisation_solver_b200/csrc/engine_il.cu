@@ -249,17 +249,6 @@ void Engine::il_set_family(int32_t family) {
     set(il64_);
 }
 
-void Engine::il_enqueue_trial(int slot, int measure) {
-    if (mixed_) {
-        launch_il_primal<float>(il32_, g_.ctl, measure, slot, stream_);
-        launch_il_dual<float>(il32_, g_.ctl, dopt_, measure, slot, stream_);
-    } else {
-        launch_il_primal<double>(il64_, g_.ctl, measure, slot, stream_);
-        launch_il_dual<double>(il64_, g_.ctl, dopt_, measure, slot, stream_);
-    }
-    launches_ += 2;
-}
-
 namespace {
 
 template <class T>

@@ -1457,6 +1457,18 @@ void launch_setup_vectors(const Global& g, const Work<T>& w, cudaStream_t s) {
     if (g.num_vec) k_setup_vectors<T><<<g.num_vec, kThreads, 0, s>>>(g, w);
 }
 
+template <class T>
+__global__ void k_fill(T* __restrict__ p, int64_t n, T v) {
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        p[k] = v;
+}
+
+template <class T>
+void launch_fill(T* p, int64_t n, T v, cudaStream_t s) {
+    if (n > 0) k_fill<T><<<static_cast<int>(std::min<int64_t>(blocks_for(n, 256), 148 * 16)), 256, 0, s>>>(p, n, v);
+}
+
 void launch_broadcast_scales(const Global& g, const InstanceInfo& first, int32_t count,
                              int64_t rows, int64_t cols, cudaStream_t s) {
     (void)first;
@@ -1552,6 +1564,7 @@ void launch_slot_done(const Global& g, int32_t count, int32_t* done, cudaStream_
     template void launch_refresh<T>(const Global&, const Work<T>&, const DeviceOptions&, int, cudaStream_t); \
     template void launch_precondition<T>(const Global&, const Work<T>&, int, int, int, int, cudaStream_t);  \
     template void launch_setup_vectors<T>(const Global&, const Work<T>&, cudaStream_t);                    \
+    template void launch_fill<T>(T*, int64_t, T, cudaStream_t);                                              \
     template void launch_broadcast_precond<T>(const Work<T>&, const InstanceInfo&, int32_t, int64_t, int64_t, cudaStream_t); \
     template void launch_spmv<T>(const Global&, int, int, const T*, T*, int, cudaStream_t);
 

@@ -122,6 +122,9 @@ void launch_precondition(const Global& g, const Work<T>& w, int enabled, int vw,
                          int at_ctas, cudaStream_t s);
 template <class T>
 void launch_setup_vectors(const Global& g, const Work<T>& w, cudaStream_t s);
+// p[0..n) = v.
+template <class T>
+void launch_fill(T* p, int64_t n, T v, cudaStream_t s);
 void launch_broadcast_scales(const Global& g, const InstanceInfo& first, int32_t count,
                              int64_t rows, int64_t cols, cudaStream_t s);
 template <class T>

@@ -65,26 +65,6 @@ std::string canonicalize(const pdlpgpu_lp& lp, HostCsr& out) {
     return std::string();
 }
 
-HostCsr transpose(const HostCsr& a) {
-    HostCsr t;
-    t.rows = a.cols;
-    t.cols = a.rows;
-    t.start.assign(static_cast<size_t>(a.cols) + 1, 0);
-    for (int32_t c : a.index) ++t.start[static_cast<size_t>(c) + 1];
-    for (int32_t j = 0; j < a.cols; ++j) t.start[j + 1] += t.start[j];
-    t.index.resize(a.index.size());
-    t.value.resize(a.value.size());
-    std::vector<int64_t> cursor(t.start.begin(), t.start.end() - 1);
-    for (int32_t i = 0; i < a.rows; ++i) {
-        for (int64_t k = a.start[i]; k < a.start[i + 1]; ++k) {
-            const int64_t pos = cursor[a.index[k]]++;
-            t.index[pos] = i;
-            t.value[pos] = a.value[k];
-        }
-    }
-    return t;
-}
-
 std::string validate_vectors(const pdlpgpu_lp& lp) {
     const int32_t m = lp.num_rows, n = lp.num_cols;
     if ((n > 0 && (lp.objective == nullptr || lp.var_lower == nullptr || lp.var_upper == nullptr)))
@@ -106,12 +86,15 @@ std::string validate_vectors(const pdlpgpu_lp& lp) {
 
 namespace {
 
+// Lines by decreasing length, ties by index: a stable counting sort.
 std::vector<int32_t> order_by_length(const std::vector<int64_t>& start, int32_t lines) {
     std::vector<int32_t> perm(static_cast<size_t>(lines));
-    std::iota(perm.begin(), perm.end(), 0);
-    std::stable_sort(perm.begin(), perm.end(), [&](int32_t x, int32_t y) {
-        return start[x + 1] - start[x] > start[y + 1] - start[y];
-    });
+    int64_t longest = 0;
+    for (int32_t x = 0; x < lines; ++x) longest = std::max(longest, start[x + 1] - start[x]);
+    std::vector<int64_t> at(static_cast<size_t>(longest) + 2, 0);   // at[longest - len + 1]: count
+    for (int32_t x = 0; x < lines; ++x) ++at[static_cast<size_t>(longest - (start[x + 1] - start[x])) + 1];
+    for (size_t k = 1; k < at.size(); ++k) at[k] += at[k - 1];
+    for (int32_t x = 0; x < lines; ++x) perm[at[static_cast<size_t>(longest - (start[x + 1] - start[x]))]++] = x;
     return perm;
 }
 
@@ -123,23 +106,37 @@ int lane_group(int64_t len, int target) {
     return g;
 }
 
-// Lines are given in internal order as (internal index, value) lists.
-void make_side(const std::vector<std::vector<std::pair<int32_t, double>>>& lines, const Tuning& t,
-               SideLayout& side) {
-    const int V = t.vector_width;
-    const int32_t L = static_cast<int32_t>(lines.size());
-    side.slices.clear();
-    side.line_len.resize(static_cast<size_t>(L));
-    int64_t total = 0;
-    for (int32_t i = 0; i < L; ++i) {
-        side.line_len[i] = static_cast<int32_t>(lines[i].size());
-        total += side.line_len[i];
+// Slice shapes of one side from its line lengths (internal order), and for
+// every line where its entries go: entry k of line i lands in slot
+// base[i] + (s / V) * 32 * V + (lane0[i] + (k & (G - 1))) * V + s % V with
+// s = k >> glog[i], G = 1 << glog[i].
+struct SlotMap {
+    std::vector<int64_t> base;
+    std::vector<int32_t> lane0;
+    std::vector<uint8_t> glog;
+    int vlog = 0;   // V = 1 << vlog
+    int64_t slot(int32_t line, int64_t k) const {
+        const int gl = glog[static_cast<size_t>(line)];
+        const int64_t s = k >> gl;
+        const int64_t lane = lane0[static_cast<size_t>(line)] + (k & ((int64_t(1) << gl) - 1));
+        return base[static_cast<size_t>(line)] + (((s >> vlog) * 32 + lane) << vlog) + (s & ((1 << vlog) - 1));
     }
-    side.entries = total;
-    // First pass: slice shapes and slot count.
+};
+
+SlotMap plan_side(std::vector<int32_t> line_len, const Tuning& t, SideLayout& side) {
+    const int V = t.vector_width;
+    const int32_t L = static_cast<int32_t>(line_len.size());
+    side.slices.clear();
+    side.entries = 0;
+    for (int32_t len : line_len) side.entries += len;
+    SlotMap map;
+    while ((1 << map.vlog) < V) ++map.vlog;
+    map.base.resize(static_cast<size_t>(L));
+    map.lane0.resize(static_cast<size_t>(L));
+    map.glog.resize(static_cast<size_t>(L));
     int64_t slots = 0;
     for (int32_t i = 0; i < L;) {
-        const int64_t len0 = side.line_len[i];
+        const int64_t len0 = line_len[i];
         const int G = lane_group(len0, t.lane_elements);
         int glog = 0;
         while ((1 << glog) < G) ++glog;
@@ -153,60 +150,69 @@ void make_side(const std::vector<std::vector<std::pair<int32_t, double>>>& lines
         sd.steps = static_cast<int32_t>(steps);
         sd.meta = glog | (nl << 8);
         side.slices.push_back(sd);
+        for (int r = 0; r < nl; ++r) {
+            map.base[static_cast<size_t>(i + r)] = slots;
+            map.lane0[static_cast<size_t>(i + r)] = r * G;
+            map.glog[static_cast<size_t>(i + r)] = static_cast<uint8_t>(glog);
+        }
         slots += steps * 32;
         i += nl;
     }
+    side.line_len = std::move(line_len);
     side.idx.assign(static_cast<size_t>(slots), 0);
     side.val.assign(static_cast<size_t>(slots), 0.0);
-    for (const SliceDesc& sd : side.slices) {
-        const int glog = slice_glog(sd.meta), nl = slice_lines(sd.meta);
-        const int G = 1 << glog;
-        const int64_t base = static_cast<int64_t>(sd.data_off) * 32;
-        for (int r = 0; r < nl; ++r) {
-            const auto& line = lines[sd.line0 + r];
-            for (size_t k = 0; k < line.size(); ++k) {
-                const int64_t s = static_cast<int64_t>(k) >> glog;
-                const int g = static_cast<int>(k) & (G - 1);
-                const int lane = r * G + g;
-                const int64_t pos = base + (s / V) * 32 * V + lane * V + (s % V);
-                side.idx[pos] = line[k].first;
-                side.val[pos] = line[k].second;
-            }
-        }
-    }
+    return map;
 }
 
 }  // namespace
 
-MatrixLayout build_layout(const HostCsr& a, const HostCsr& at, const Tuning& t) {
+// One pass over the rows of A in internal order: each row's entries are
+// renumbered to internal columns and sorted (rows are short), written to
+// their A-side slots, and appended to their columns' A^T-side slots. Rows
+// are visited in increasing internal order, so every column receives its
+// entries in increasing internal row order -- no transpose of A and no
+// intermediate copy.
+MatrixLayout build_layout(const HostCsr& a, const Tuning& t) {
     MatrixLayout L;
-    L.m = a.rows;
-    L.n = a.cols;
-    L.row_perm = order_by_length(a.start, a.rows);
-    L.col_perm = order_by_length(at.start, at.rows);
-    std::vector<int32_t> inv_row(static_cast<size_t>(a.rows)), inv_col(static_cast<size_t>(a.cols));
-    for (int32_t r = 0; r < a.rows; ++r) inv_row[L.row_perm[r]] = r;
-    for (int32_t c = 0; c < a.cols; ++c) inv_col[L.col_perm[c]] = c;
-
-    std::vector<std::vector<std::pair<int32_t, double>>> lines(static_cast<size_t>(a.rows));
-    for (int32_t r = 0; r < a.rows; ++r) {
+    const int32_t m = a.rows, n = a.cols;
+    L.m = m;
+    L.n = n;
+    L.row_perm = order_by_length(a.start, m);
+    std::vector<int64_t> col_start(static_cast<size_t>(n) + 1, 0);
+    for (int32_t j : a.index) ++col_start[static_cast<size_t>(j) + 1];
+    for (int32_t j = 0; j < n; ++j) col_start[j + 1] += col_start[j];
+    L.col_perm = order_by_length(col_start, n);
+    std::vector<int32_t> inv_col(static_cast<size_t>(n));
+    std::vector<int32_t> row_len(static_cast<size_t>(m)), col_len(static_cast<size_t>(n));
+    for (int32_t c = 0; c < n; ++c) {
+        const int32_t j = L.col_perm[c];
+        inv_col[j] = c;
+        col_len[c] = static_cast<int32_t>(col_start[j + 1] - col_start[j]);
+    }
+    for (int32_t r = 0; r < m; ++r) {
         const int32_t i = L.row_perm[r];
-        auto& line = lines[r];
-        line.reserve(static_cast<size_t>(a.start[i + 1] - a.start[i]));
+        row_len[r] = static_cast<int32_t>(a.start[i + 1] - a.start[i]);
+    }
+    const SlotMap rows = plan_side(std::move(row_len), t, L.a);
+    const SlotMap cols = plan_side(std::move(col_len), t, L.at);
+    std::vector<int64_t> fill(static_cast<size_t>(n), 0);   // entries placed per column
+    std::vector<std::pair<int32_t, double>> line;
+    for (int32_t r = 0; r < m; ++r) {
+        const int32_t i = L.row_perm[r];
+        line.clear();
         for (int64_t k = a.start[i]; k < a.start[i + 1]; ++k) line.emplace_back(inv_col[a.index[k]], a.value[k]);
         std::sort(line.begin(), line.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+        for (size_t k = 0; k < line.size(); ++k) {
+            const int32_t c = line[k].first;
+            const double v = line[k].second;
+            const int64_t p = rows.slot(r, static_cast<int64_t>(k));
+            L.a.idx[static_cast<size_t>(p)] = c;
+            L.a.val[static_cast<size_t>(p)] = v;
+            const int64_t q = cols.slot(c, fill[static_cast<size_t>(c)]++);
+            L.at.idx[static_cast<size_t>(q)] = r;
+            L.at.val[static_cast<size_t>(q)] = v;
+        }
     }
-    make_side(lines, t, L.a);
-
-    lines.assign(static_cast<size_t>(a.cols), {});
-    for (int32_t c = 0; c < a.cols; ++c) {
-        const int32_t j = L.col_perm[c];
-        auto& line = lines[c];
-        line.reserve(static_cast<size_t>(at.start[j + 1] - at.start[j]));
-        for (int64_t k = at.start[j]; k < at.start[j + 1]; ++k) line.emplace_back(inv_row[at.index[k]], at.value[k]);
-        std::sort(line.begin(), line.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
-    }
-    make_side(lines, t, L.at);
     return L;
 }
 
@@ -242,10 +248,10 @@ int64_t cta_target_slots(int64_t slots, int sms) {
     return std::max<int64_t>(256, std::min<int64_t>(per, 65536));
 }
 
-Tuning choose_tuning(const HostCsr& a, const HostCsr& at, bool fp32) {
+Tuning choose_tuning(const HostCsr& a, bool fp32) {
     Tuning t;
     const double mean_a = a.rows ? static_cast<double>(a.nnz()) / a.rows : 0.0;
-    const double mean_at = at.rows ? static_cast<double>(at.nnz()) / at.rows : 0.0;
+    const double mean_at = a.cols ? static_cast<double>(a.nnz()) / a.cols : 0.0;
     const double mean = std::min(mean_a, mean_at);
     t.lane_elements = 8;
     if (fp32) t.vector_width = mean >= 24.0 ? 4 : (mean >= 12.0 ? 2 : 1);

@@ -26,9 +26,6 @@ struct HostCsr {
 // empty string, or the reference's exception message for invalid input.
 std::string canonicalize(const pdlpgpu_lp& lp, HostCsr& out);
 
-// CSR of A^T by counting sort over the rows of A (sparse_matrix.cpp:171-198).
-HostCsr transpose(const HostCsr& a);
-
 // CompiledLp::validate (pdlp_engine/include/pdlp/compiled_lp.h:32-62) on the
 // vectors. Returns an empty string or the reference's message.
 std::string validate_vectors(const pdlpgpu_lp& lp);
@@ -58,7 +55,7 @@ struct MatrixLayout {
 
 // Renumbers rows by decreasing length and columns by decreasing degree (ties
 // by original index), then builds both sides.
-MatrixLayout build_layout(const HostCsr& a, const HostCsr& at, const Tuning& t);
+MatrixLayout build_layout(const HostCsr& a, const Tuning& t);
 
 // Splits the slices of each instance into CTAs of roughly `target_slots`
 // slots (never crossing an instance). Appends to `out`; returns the count.
@@ -72,6 +69,6 @@ int append_vec_map(int32_t instance, int32_t m, int32_t n, std::vector<VecWork>&
 int64_t cta_target_slots(int64_t slots, int sms);
 
 // Autotuning heuristic for a matrix: lane target and vector width.
-Tuning choose_tuning(const HostCsr& a, const HostCsr& at, bool fp32);
+Tuning choose_tuning(const HostCsr& a, bool fp32);
 
 }  // namespace pdlpgpu

@@ -28,7 +28,11 @@ def _to_result(r: native.Result) -> PdlpResult:
     n, m = r.num_cols, r.num_rows
 
     def arr(p, k):
-        return np.ctypeslib.as_array(p, shape=(k,)).copy() if p and k > 0 else np.zeros(0)
+        if not p or k <= 0:
+            return np.zeros(0)
+        a = np.empty(k)
+        C.memmove(a.ctypes.data, p, a.nbytes)
+        return a
 
     return PdlpResult(
         status=PdlpStatus(r.status), status_message=r.status_message.decode(),
