@@ -90,11 +90,15 @@ __device__ __forceinline__ LanePos lane_pos(const SliceDesc& sd, int lane) {
 // bits, so the result is deterministic). Up to kDepth vector loads of index
 // and value are issued before their gathers, so a lane keeps several
 // independent memory requests in flight instead of one load-gather chain.
-template <int V, int NQ, class TA, class TV, class F>
+// kDeep doubles the depth for FP32 vector loads (measured: the dual kernel
+// gains, the primal kernel, whose lanes also stream five vectors, loses).
+template <int V, int NQ, bool kDeep = false, class TA, class TV, class F>
 __device__ __forceinline__ void line_sums(int64_t base, int steps, const LanePos& lp, int lane,
                                           int len, const int32_t* __restrict__ idx,
                                           const TV* __restrict__ val, TA (&acc)[NQ], F fetch) {
-    constexpr int kDepth = V >= 4 ? 1 : 4 / V;   // about four entries in flight per lane
+    // About four entries in flight per lane, eight for deep FP32 vector
+    // loads (deeper FP64 or scalar pipelines spill at 64 registers).
+    constexpr int kDepth = (kDeep && V >= 2 && sizeof(TV) == 4) ? 8 / V : (V >= 4 ? 1 : 4 / V);
     constexpr int kStep = kDepth * V;
     // Software pipeline: the index and value loads of the next group are in
     // flight while the current group's gathers are.
@@ -314,9 +318,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_dual(Global g, Work<T> w, Devic
             if (pending) ai = avg[i];
         }
         T sum[1] = {T(0)};
-        line_sums<V, 1>(inf.a_data_base + static_cast<int64_t>(sd.data_off) * 32, sd.steps, lp,
-                        lane, len, g.a.idx, vals, sum,
-                        [&](T (&a)[1], T v, int j) { a[0] += v * xt[j]; });
+        line_sums<V, 1, true>(inf.a_data_base + static_cast<int64_t>(sd.data_off) * 32, sd.steps, lp,
+                              lane, len, g.a.idx, vals, sum,
+                              [&](T (&a)[1], T v, int j) { a[0] += v * xt[j]; });
         if (owner) {
             const T next = sum[0];
             const T dact = next - axi;

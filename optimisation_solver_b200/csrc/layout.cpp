@@ -245,7 +245,7 @@ int append_vec_map(int32_t instance, int32_t m, int32_t n, std::vector<VecWork>&
 
 int64_t cta_target_slots(int64_t slots, int sms) {
     const int64_t per = slots / (static_cast<int64_t>(sms) * 8);
-    return std::max<int64_t>(256, std::min<int64_t>(per, 65536));
+    return std::max<int64_t>(256, std::min<int64_t>(per, 32768));
 }
 
 Tuning choose_tuning(const HostCsr& a, bool fp32) {
