@@ -27,17 +27,22 @@ constexpr int kIlThreads = kIlWarps * 32;
 
 // True in every thread of the CTA that arrives last of `expected` CTAs
 // (and resets the counter). Everything written before is visible to it.
+// One thread fences for the CTA: the barrier orders the other threads'
+// writes before its fence, and a fence covers the writes its thread has
+// observed (the pattern of a cooperative grid barrier).
 __device__ __forceinline__ bool arrive_last_cta(int32_t* counter, int expected) {
     __shared__ int last;
-    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
+        __threadfence();
         const int prev = atomicAdd(counter, 1);
         last = prev == expected - 1;
-        if (last) *counter = 0;
+        if (last) {
+            *counter = 0;
+            __threadfence();
+        }
     }
     __syncthreads();
-    if (last) __threadfence();
     return last != 0;
 }
 
@@ -733,6 +738,7 @@ template <class T, int V, bool kFam>
 __global__ void __launch_bounds__(kIlThreads, 3) k_il_dual(Interleaved<T> il, InstanceCtl* ctl,
                                                            DeviceOptions o, int measure, int slot) {
     constexpr int G = 32 * V;
+    static_assert(kIlThreads >= 2 * G, "the decision adds its two sums in two halves of the CTA");
     // The lane states are read before the first tile is staged (the barrier
     // in lane_state orders them), so they share the stage's memory.
     __shared__ union Smem {
@@ -807,18 +813,30 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_dual(Interleaved<T> il, In
     // The options by reference from shared memory: a reference to the kernel
     // parameter would make every thread of every CTA copy it to local memory.
     __shared__ DeviceOptions so;
+    __shared__ double primal_sum[G];
     if (t == 0) so = o;
+    // The instance's hot block and the group's two sums are fetched at
+    // once: threads [0, G) add the dual kernel's batch sums of instance t,
+    // threads [G, 2G) the primal kernel's of instance t - G.
+    const int b = static_cast<int>(gp * G) + t;
+    const bool mine = t < G && b < il.count;
+    HotCtl h{};
+    if (mine) h = load_hot(ctl + b);
+    double dd[2] = {0.0, 0.0};
+    if (t < G) {
+        sum_batches<2, G>(il.part2_dual + gp * il.row_batches * 2 * G, il.row_batches, t, dd);
+    } else if (t < 2 * G) {
+        double pm[1];
+        sum_batches<1, G>(il.part2_primal + gp * il.col_batches * G, il.col_batches, t - G, pm);
+        primal_sum[t - G] = pm[0];
+    }
     __syncthreads();
     // The linesearch decision of each instance of the group (one thread each).
-    const int b = static_cast<int>(gp * G) + t;
-    if (t >= G || b >= il.count) return;
+    if (!mine) return;
+    if (h.phase == kPhaseDone || h.stage != kStageTrial || (h.fp64 != 0) != (sizeof(T) == 8)) return;
     InstanceCtl& c = ctl[b];
-    if (!trial_active<T>(c)) return;
-    double pm[1], dd[2];
-    sum_batches<1, G>(il.part2_primal + gp * il.col_batches * G, il.col_batches, t, pm);
-    sum_batches<2, G>(il.part2_dual + gp * il.row_batches * 2 * G, il.row_batches, t, dd);
     const int before = c.parity;
-    trial_control(c, so, pm[0], dd[0], dd[1], il.n);
+    trial_control(c, so, primal_sum[t], dd[0], dd[1], il.n);
     c.ibuf = c.parity != before ? W : R;
 }
 

@@ -185,18 +185,22 @@ __device__ __forceinline__ double warp_range_sum(const double* part, int begin, 
 
 // Arrival counter: returns true in every thread of the CTA that arrives last
 // among `expected` CTAs of the instance (and resets the counter for the next
-// launch). Partials written before the call are visible to that CTA.
+// launch). Partials written before the call are visible to that CTA. One
+// thread fences for the CTA: the barrier orders the other threads' writes
+// before its fence, which covers the writes its thread has observed.
 __device__ __forceinline__ bool arrive_last(int32_t* counter, int expected) {
     __shared__ int last;
-    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
+        __threadfence();
         const int prev = atomicAdd(counter, 1);
         last = prev == expected - 1;
-        if (last) *counter = 0;
+        if (last) {
+            *counter = 0;
+            __threadfence();
+        }
     }
     __syncthreads();
-    if (last) __threadfence();
     return last != 0;
 }
 
