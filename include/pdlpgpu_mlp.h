@@ -15,6 +15,10 @@
  *   outputs  [batch][out]  FP32
  *   targets  [batch][out]  FP32, with per-output loss weights [out]
  * `in` must be a multiple of 8; `out` and `hidden` multiples of 64.
+ * The model runs on its own stream, ordered after all work enqueued so far
+ * on the legacy default stream (where the codec below and PyTorch enqueue
+ * by default); arguments produced on another stream must be complete before
+ * the call. Each call returns once its results are written.
  */
 #ifndef PDLPGPU_MLP_H
 #define PDLPGPU_MLP_H

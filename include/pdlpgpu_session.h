@@ -33,7 +33,12 @@ void pdlpgpu_session_destroy(pdlpgpu_session* session);
 
 /* Per-instance vectors, row-major [batch][n] or [batch][m], original order.
  * NULL keeps the family's vector for every instance. `on_device` = 1 means the
- * pointers are device memory on the session's GPU (nothing crosses PCIe).
+ * pointers are device memory on the session's GPU (nothing crosses PCIe);
+ * the session reads and writes such buffers only after all work enqueued so
+ * far on the legacy default stream (CUDA's stream 0, where PyTorch enqueues
+ * by default), so data produced there needs no synchronisation; data
+ * produced on any other stream must be complete before the call. The same
+ * holds for the device buffers of pdlpgpu_session_read and _stream.
  * warm_primal / warm_dual / warm_weight enable a warm start for every
  * instance (original coordinates, PDLP dual sign; weight <= 0 = default);
  * the better of warm and cold start by KKT score is used per instance. */

@@ -230,6 +230,7 @@ bool Engine::upload(void* dst, const std::vector<HostPiece>& pieces) {
 Engine::~Engine() {
     for (cudaEvent_t e : tev_)
         if (e) cudaEventDestroy(e);
+    if (caller_done_) cudaEventDestroy(caller_done_);
     for (void* q : extra_) cudaFree(q);
     if (graph_) cudaGraphExecDestroy(graph_);
     if (graph64_) cudaGraphExecDestroy(graph64_);
@@ -1386,10 +1387,24 @@ bool Engine::session_create(const pdlpgpu_lp& family, int32_t batch, const pdlpg
     return check(cudaStreamSynchronize(stream_), "session setup");
 }
 
+// Device-pointer inputs are usually written just before the call by the
+// caller's own kernels or copies, enqueued on the legacy default stream (the
+// stream PyTorch and most callers use by default). The session's stream does
+// not synchronise with it implicitly (it is non-blocking), so it waits for
+// everything enqueued there so far.
+bool Engine::wait_for_caller() {
+    if (caller_done_ == nullptr &&
+        !check(cudaEventCreateWithFlags(&caller_done_, cudaEventDisableTiming), "cudaEventCreate"))
+        return false;
+    return check(cudaEventRecord(caller_done_, cudaStreamLegacy), "cudaEventRecord") &&
+           check(cudaStreamWaitEvent(stream_, caller_done_, 0), "cudaStreamWaitEvent");
+}
+
 bool Engine::session_load(bool on_device, const double* c, const double* rl, const double* ru,
                           const double* xl, const double* xu, const double* wx, const double* wy,
                           const double* ww) {
     const int64_t n = info_[0].n, m = info_[0].m;
+    if (on_device && !wait_for_caller()) return false;
     auto load = [&](const double* src, double* dst, const double* fam, bool cols) {
         const int64_t len = cols ? n : m;
         if (src == nullptr) {
@@ -1468,6 +1483,7 @@ bool Engine::session_solve(int32_t* optimal) {
 bool Engine::session_read(bool on_device, double* primal, double* dual, int32_t* status,
                           int64_t* iterations, double* stats) {
     const int64_t n = info_[0].n, m = info_[0].m;
+    if (on_device && (primal != nullptr || dual != nullptr) && !wait_for_caller()) return false;
     if (primal != nullptr) {
         double* dst = on_device ? primal : g_.x_o;
         launch_permute(g_.best_x, dst, d_col_perm_, n, count_, 1, stream_);
@@ -1594,6 +1610,7 @@ bool Engine::session_stream(bool on_device, int64_t N, const double* const in[5]
     const int32_t B = count_;
     const int64_t n = info_[0].n, m = info_[0].m;
     const pdlpgpu_options& o = spec_.opt;
+    if (on_device && !wait_for_caller()) return false;
     std::vector<void*> temp;   // per-call device buffers
     auto dalloc = [&](auto*& p, size_t count, std::vector<void*>& list) {
         void* q = nullptr;

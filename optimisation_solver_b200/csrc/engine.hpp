@@ -201,6 +201,10 @@ private:
     // last): [3 + 3p] trial start, [4 + 3p] between the halves, [5 + 3p] end
     static constexpr int kTimedSlots = 4;
     cudaEvent_t tev_[3 + 3 * kTimedSlots] = {};
+    // Orders the session's stream after the caller's work on the legacy
+    // default stream before device-pointer inputs are read.
+    bool wait_for_caller();
+    cudaEvent_t caller_done_ = nullptr;
     double t_primal_[kTimedSlots] = {}, t_dual_[kTimedSlots] = {};
     double t_chunk_ = 0.0, t_check_ = 0.0;
     int64_t t_samples_ = 0, t_chunks_ = 0;

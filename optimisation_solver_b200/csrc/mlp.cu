@@ -514,6 +514,7 @@ using namespace pdlpgpu_mlp_impl;
 struct pdlpgpu_mlp {
     int in = 0, hidden = 0, out = 0, batch = 0, device = 0;
     cudaStream_t stream = nullptr;
+    cudaEvent_t caller_done = nullptr;
     std::vector<void*> allocs;
     // parameters (FP32 master), BF16 copies, Adam moments, gradients
     float *W1 = nullptr, *b1 = nullptr, *W2 = nullptr, *b2 = nullptr, *W3 = nullptr, *b3 = nullptr;
@@ -536,7 +537,21 @@ struct pdlpgpu_mlp {
 
     ~pdlpgpu_mlp() {
         for (void* p : allocs) cudaFree(p);
+        if (caller_done) cudaEventDestroy(caller_done);
         if (stream) cudaStreamDestroy(stream);
+    }
+
+    // The caller's device arguments (features, targets, parameters) are
+    // usually written just before the call on the legacy default stream --
+    // by pdlpgpu_encode_features, or by PyTorch, which enqueues there by
+    // default -- and the model's own stream does not synchronise with it
+    // implicitly (it is non-blocking): it waits for all work enqueued there
+    // so far before it reads them.
+    bool wait_for_caller() {
+        if (!caller_done && cudaEventCreateWithFlags(&caller_done, cudaEventDisableTiming) != cudaSuccess)
+            return false;
+        return cudaEventRecord(caller_done, cudaStreamLegacy) == cudaSuccess &&
+               cudaStreamWaitEvent(stream, caller_done, 0) == cudaSuccess;
     }
 
     template <class T>
@@ -742,6 +757,7 @@ int32_t pdlpgpu_mlp_forward(pdlpgpu_mlp* m, const uint16_t* inputs, float* outpu
     if (!m) return -1;
     cudaSetDevice(m->device);
     m->launches = 0;
+    if (!m->wait_for_caller()) return fail("mlp forward: stream wait failed");
     if (!m->forward(reinterpret_cast<const bf16*>(inputs))) return fail("mlp forward: " + m->msg);
     if (cudaMemcpyAsync(outputs, m->Out, sizeof(float) * m->batch * m->out, cudaMemcpyDeviceToDevice,
                         m->stream) != cudaSuccess)
@@ -756,6 +772,7 @@ int32_t pdlpgpu_mlp_gradients(pdlpgpu_mlp* m, const uint16_t* inputs, const floa
     if (!m) return -1;
     cudaSetDevice(m->device);
     m->launches = 0;
+    if (!m->wait_for_caller()) return fail("mlp gradients: stream wait failed");
     const bf16* X = reinterpret_cast<const bf16*>(inputs);
     if (!m->forward(X) || !m->backward(X, targets, w)) return fail("mlp gradients: " + m->msg);
     const int64_t H = m->hidden, I = m->in, O = m->out;
@@ -774,6 +791,7 @@ int32_t pdlpgpu_mlp_train_step(pdlpgpu_mlp* m, const uint16_t* inputs, const flo
     if (!m) return -1;
     cudaSetDevice(m->device);
     m->launches = 0;
+    if (!m->wait_for_caller()) return fail("mlp train: stream wait failed");
     const bf16* X = reinterpret_cast<const bf16*>(inputs);
     if (!m->forward(X) || !m->backward(X, targets, w)) return fail("mlp train: " + m->msg);
     m->adam_all(lr);
@@ -785,6 +803,8 @@ int32_t pdlpgpu_mlp_train_step(pdlpgpu_mlp* m, const uint16_t* inputs, const flo
 int32_t pdlpgpu_mlp_get_params(pdlpgpu_mlp* m, float* W1, float* b1, float* W2, float* b2,
                                float* W3, float* b3) {
     if (!m) return -1;
+    cudaSetDevice(m->device);
+    if (!m->wait_for_caller()) return fail("mlp get_params: stream wait failed");
     const int64_t H = m->hidden, I = m->in, O = m->out;
     auto cp = [&](float* dst, const float* src, int64_t n) {
         if (dst) cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyDeviceToDevice, m->stream);
@@ -797,6 +817,8 @@ int32_t pdlpgpu_mlp_get_params(pdlpgpu_mlp* m, float* W1, float* b1, float* W2, 
 int32_t pdlpgpu_mlp_set_params(pdlpgpu_mlp* m, const float* W1, const float* b1, const float* W2,
                                const float* b2, const float* W3, const float* b3) {
     if (!m) return -1;
+    cudaSetDevice(m->device);
+    if (!m->wait_for_caller()) return fail("mlp set_params: stream wait failed");
     const int64_t H = m->hidden, I = m->in, O = m->out;
     auto cp = [&](float* dst, const float* src, int64_t n) {
         if (src) cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyDeviceToDevice, m->stream);

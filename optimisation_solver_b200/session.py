@@ -8,6 +8,7 @@ instance to completion on the device.
 from __future__ import annotations
 
 import ctypes as C
+import sys
 
 import numpy as np
 
@@ -16,6 +17,18 @@ from .lp import CompiledLp, PdlpOptions, PdlpStatus
 
 _PRECISIONS = {"fp64": 0, "mixed": 1}
 _LAYOUTS = {"auto": 0, "sell": 1, "interleaved": 2}
+
+
+def _caller_stream_done():
+    """Device-pointer arguments are ordered after the caller's work on the
+    legacy default stream by the library itself; a caller that enqueued
+    them on another PyTorch stream is waited for here."""
+    torch = sys.modules.get("torch")
+    if torch is None or not torch.cuda.is_initialized():
+        return
+    current = torch.cuda.current_stream()
+    if current != torch.cuda.default_stream(current.device):
+        current.synchronize()
 
 
 def _addr(a):
@@ -68,6 +81,8 @@ class Session:
                 warm_weight]
         if not on_device:
             arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
+        else:
+            _caller_stream_done()
         self._keep = arrs
         rc = native.lib().pdlpgpu_session_load(self._s, int(on_device), *[_addr(a) for a in arrs])
         if rc != 0:
@@ -87,6 +102,8 @@ class Session:
                 primal = np.zeros((self.batch, self.n))
             if dual is None:
                 dual = np.zeros((self.batch, self.m))
+        else:
+            _caller_stream_done()
         status = np.zeros(self.batch, dtype=np.int32)
         iters = np.zeros(self.batch, dtype=np.int64)
         stats = np.zeros((self.batch, 8))
@@ -115,6 +132,8 @@ class Session:
                 primal = np.zeros((count, self.n))
             if dual is None:
                 dual = np.zeros((count, self.m))
+        else:
+            _caller_stream_done()
         status = np.zeros(count, dtype=np.int32)
         iters = np.zeros(count, dtype=np.int64)
         stats = np.zeros((count, 8))

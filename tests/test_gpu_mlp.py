@@ -67,6 +67,29 @@ def test_forward_matches_oracle():
     assert np.linalg.norm(got - want) <= 1e-2 * np.linalg.norm(want)
 
 
+def test_forward_waits_for_inputs_written_just_before():
+    """Features still being copied in on the default stream, behind tens of
+    milliseconds of other work, when the forward pass is called: the model
+    waits for them, and its outputs are those of resident inputs."""
+    import torch
+    net, X, T, w, P = _small_net(2)
+    ref = torch.empty((net.batch, net.outputs), dtype=torch.float32, device="cuda")
+    x_ready = _bf(X)
+    torch.cuda.synchronize()
+    net.forward(x_ready, ref)
+    x_late = torch.full_like(x_ready, float("nan"))
+    x_host = x_ready.cpu().pin_memory()
+    torch.cuda.synchronize()
+    busy = torch.randn((4096, 4096), device="cuda")
+    for _ in range(40):
+        busy = torch.tanh(busy @ busy)
+    x_late.copy_(x_host, non_blocking=True)
+    out = torch.empty_like(ref)
+    net.forward(x_late, out)
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref)
+
+
 def test_gradients_match_oracle():
     import torch
     net, X, T, w, P = _small_net(2)

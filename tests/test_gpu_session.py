@@ -88,6 +88,36 @@ def test_device_pointers_match_host_arrays(family, layout):
     assert np.array_equal(py.cpu().numpy(), host["dual"])
 
 
+def test_device_inputs_written_just_before_the_call(family):
+    """Device inputs whose values are still being written by the caller's
+    kernels on the default stream when the stream call is made (behind a
+    long chain of matrix products): the session waits for them, so the
+    results are those of the same instances passed as host arrays."""
+    import torch
+    G, fam, s, c = family
+    opts = PdlpOptions().with_tolerance(1e-4)
+    S = Session(fam, 16, opts, precision="mixed")
+    host = S.stream(24, objective=c[:24], row_lower=s[:24], row_upper=s[:24])
+    sd = torch.full((24, fam.num_rows), float("nan"), dtype=torch.float64, device="cuda")
+    cd = torch.full((24, fam.num_cols), float("nan"), dtype=torch.float64, device="cuda")
+    px = torch.empty((24, fam.num_cols), dtype=torch.float64, device="cuda")
+    py = torch.empty((24, fam.num_rows), dtype=torch.float64, device="cuda")
+    s_h = torch.as_tensor(s[:24]).pin_memory()
+    c_h = torch.as_tensor(c[:24]).pin_memory()
+    torch.cuda.synchronize()
+    busy = torch.randn((4096, 4096), device="cuda")
+    for _ in range(40):          # tens of milliseconds of default-stream work
+        busy = torch.tanh(busy @ busy)
+    sd.copy_(s_h, non_blocking=True)
+    cd.copy_(c_h, non_blocking=True)
+    dev = S.stream(24, objective=cd, row_lower=sd, row_upper=sd, primal=px, dual=py, on_device=True)
+    torch.cuda.synchronize()
+    assert dev["optimal"] == host["optimal"] == 24
+    assert np.array_equal(dev["iterations"], host["iterations"])
+    assert np.array_equal(px.cpu().numpy(), host["primal"])
+    assert np.array_equal(py.cpu().numpy(), host["dual"])
+
+
 @pytest.mark.parametrize("layout", LAYOUTS)
 def test_warm_start_from_solution_converges_fast(family, layout):
     G, fam, s, c = family
