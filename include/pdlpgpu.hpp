@@ -16,6 +16,7 @@
 #include "pdlp/pdlp_result.h"
 #include "pdlpgpu.h"
 
+#include <cstddef>
 #include <cstdint>
 #include <vector>
 
@@ -30,6 +31,24 @@ public:
 
     pdlp::PdlpResult solve(const pdlp::CompiledLp& problem,
                            const pdlp::PdlpOptions& options = {}) const {
+        // The C ABI carries the vectors as bare pointers, so the checks that
+        // need their lengths run here, in CompiledLp::validate's order
+        // (pdlp_engine/include/pdlp/compiled_lp.h:32-45); the engine checks
+        // the rest.
+        auto reject = [](const char* message) {
+            pdlp::PdlpResult out;   // defaults are the invalid-problem result
+            out.status = pdlp::PdlpStatus::InvalidProblem;
+            out.statusMessage = message;
+            return out;
+        };
+        const std::size_t n = static_cast<std::size_t>(problem.numColumns());
+        const std::size_t m = static_cast<std::size_t>(problem.numRows());
+        if (!problem.matrix.validate()) return reject("CompiledLp contains an invalid sparse matrix");
+        if (problem.objective.size() != n || problem.variableLower.size() != n ||
+            problem.variableUpper.size() != n)
+            return reject("CompiledLp column vector dimensions do not match A");
+        if (problem.rowLower.size() != m || problem.rowUpper.size() != m)
+            return reject("CompiledLp row vector dimensions do not match A");
         const pdlp::SparseMatrix& a = problem.matrix;
         pdlpgpu_lp lp;
         lp.num_rows = problem.numRows();
