@@ -164,21 +164,37 @@ def ptr(a, ctype=C.c_double):
 
 
 class LpHandle:
-    """Holds the contiguous arrays of one LP alive while the C struct is used."""
+    """Holds the contiguous arrays of one LP alive while the C struct is used.
+
+    The C ABI receives bare pointers, so lengths are checked here: a vector
+    whose length does not match A is passed as NULL, which the library
+    rejects with the reference's dimension message, and an inconsistent CSR
+    (row_start not of length rows + 1, or fewer entries than it claims) is
+    passed with a NULL row_start ("CompiledLp contains an invalid sparse
+    matrix") -- never an array the library would read past its end."""
 
     def __init__(self, lp):
+        m, n = int(lp.num_rows), int(lp.num_cols)
         self.row_start = np.ascontiguousarray(lp.row_start, dtype=np.int64)
         self.col_index = np.ascontiguousarray(lp.col_index, dtype=np.int32)
         self.values = np.ascontiguousarray(lp.values, dtype=np.float64)
-        self.objective = np.ascontiguousarray(lp.objective, dtype=np.float64)
-        self.row_lower = np.ascontiguousarray(lp.row_lower, dtype=np.float64)
-        self.row_upper = np.ascontiguousarray(lp.row_upper, dtype=np.float64)
-        self.var_lower = np.ascontiguousarray(lp.var_lower, dtype=np.float64)
-        self.var_upper = np.ascontiguousarray(lp.var_upper, dtype=np.float64)
-        self.struct = Lp(int(lp.num_rows), int(lp.num_cols), ptr(self.row_start, C.c_int64),
-                         ptr(self.col_index, C.c_int32), ptr(self.values), ptr(self.objective),
-                         float(lp.objective_offset), ptr(self.row_lower), ptr(self.row_upper),
-                         ptr(self.var_lower), ptr(self.var_upper))
+
+        def vec(a, k):
+            v = np.ascontiguousarray(a, dtype=np.float64)
+            return v if v.ndim == 1 and v.shape[0] == k else None
+
+        self.objective = vec(lp.objective, n)
+        self.row_lower = vec(lp.row_lower, m)
+        self.row_upper = vec(lp.row_upper, m)
+        self.var_lower = vec(lp.var_lower, n)
+        self.var_upper = vec(lp.var_upper, n)
+        csr_ok = (m >= 0 and self.row_start.ndim == 1 and self.row_start.shape[0] == m + 1 and
+                  self.col_index.shape[0] == self.values.shape[0] and
+                  0 <= int(self.row_start[-1]) <= self.values.shape[0])
+        starts = ptr(self.row_start, C.c_int64) if csr_ok else None
+        self.struct = Lp(m, n, starts, ptr(self.col_index, C.c_int32), ptr(self.values),
+                         ptr(self.objective), float(lp.objective_offset), ptr(self.row_lower),
+                         ptr(self.row_upper), ptr(self.var_lower), ptr(self.var_upper))
 
 
 def options_struct(options) -> Options:

@@ -59,3 +59,30 @@ def test_invalid_problem_needs_no_device():
     assert r.status == PdlpStatus.INVALID_PROBLEM
     assert r.status_message == "Invalid row bounds"
     assert r.primal.size == 0 and np.isnan(r.primal_objective)
+
+
+def test_mis_sized_vectors_are_rejected_not_read():
+    """A CompiledLp whose vectors or CSR arrays do not match its dimensions
+    gets the reference's message (compiled_lp.h:32-45), decided on the host;
+    the library is never handed an array shorter than it would read."""
+    import dataclasses
+
+    from optimisation_solver_b200.lp import PdlpStatus, SparseMatrix
+    from optimisation_solver_b200.pdlp import PdlpSolver
+    base = cases.infeasible_rows()
+    solver = PdlpSolver()
+    expect = {
+        "objective": "CompiledLp column vector dimensions do not match A",
+        "var_upper": "CompiledLp column vector dimensions do not match A",
+        "row_lower": "CompiledLp row vector dimensions do not match A",
+        "row_upper": "CompiledLp row vector dimensions do not match A",
+    }
+    for field, message in expect.items():
+        lp = dataclasses.replace(base, **{field: np.asarray(getattr(base, field))[:-1]})
+        r = solver.solve(lp, cases.strict_options())
+        assert r.status == PdlpStatus.INVALID_PROBLEM and r.status_message == message, field
+    m = base.matrix
+    short = SparseMatrix(m.rows, m.columns, m.row_start, m.col_index[:-1], m.values[:-1])
+    r = solver.solve(dataclasses.replace(base, matrix=short), cases.strict_options())
+    assert r.status == PdlpStatus.INVALID_PROBLEM
+    assert r.status_message == "CompiledLp contains an invalid sparse matrix"
