@@ -31,6 +31,23 @@ def _caller_stream_done():
         current.synchronize()
 
 
+def _check_sizes(arrs, rows, n, m):
+    """The library reads rows x length elements of each per-instance input
+    (objective, row bounds, variable bounds, warm primal, warm dual, warm
+    weight), the first rows of a larger one: an array or tensor with fewer
+    elements is refused here rather than read past its end. Raw integer
+    device pointers are the caller's responsibility."""
+    names = ("objective", "row_lower", "row_upper", "var_lower", "var_upper", "warm_primal",
+             "warm_dual", "warm_weight")
+    lengths = (n, m, m, n, n, n, m, 1)
+    for a, name, k in zip(arrs, names, lengths):
+        if a is None or isinstance(a, int):
+            continue
+        size = a.numel() if hasattr(a, "numel") else np.size(a)
+        if size < rows * k:
+            raise ValueError(f"{name}: {size} elements, at least {rows} x {k} expected")
+
+
 def _addr(a):
     """Address of a host numpy array, an integer device pointer, a CUDA tensor, or None."""
     if a is None:
@@ -79,6 +96,7 @@ class Session:
              on_device: bool = False):
         arrs = [objective, row_lower, row_upper, var_lower, var_upper, warm_primal, warm_dual,
                 warm_weight]
+        _check_sizes(arrs, self.batch, self.n, self.m)
         if not on_device:
             arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
         else:
@@ -126,6 +144,7 @@ class Session:
         writes into the given device buffers (or none)."""
         arrs = [objective, row_lower, row_upper, var_lower, var_upper, warm_primal, warm_dual,
                 warm_weight]
+        _check_sizes(arrs, int(count), self.n, self.m)
         if not on_device:
             arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
             if primal is None:

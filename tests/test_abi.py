@@ -86,3 +86,19 @@ def test_mis_sized_vectors_are_rejected_not_read():
     r = solver.solve(dataclasses.replace(base, matrix=short), cases.strict_options())
     assert r.status == PdlpStatus.INVALID_PROBLEM
     assert r.status_message == "CompiledLp contains an invalid sparse matrix"
+
+
+def test_session_refuses_short_inputs_before_any_device_work():
+    """Per-instance inputs shorter than the instances x length the library
+    would read are refused by the Python session before the C call."""
+    import pytest
+
+    from optimisation_solver_b200.session import _check_sizes
+    n, m = 5, 3
+    ok = [np.zeros((4, n)), np.zeros((4, m)), None, None, None, None, None, np.zeros(4)]
+    _check_sizes(ok, 4, n, m)
+    _check_sizes([np.zeros((6, n))] + [None] * 7, 4, n, m)   # extra rows are not read
+    with pytest.raises(ValueError, match="row_lower"):
+        _check_sizes([None, np.zeros((3, m))] + [None] * 6, 4, n, m)
+    with pytest.raises(ValueError, match="warm_weight"):
+        _check_sizes([None] * 7 + [np.zeros(3)], 4, n, m)
