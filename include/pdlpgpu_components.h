@@ -53,8 +53,11 @@ int32_t pdlpgpu_trial(const pdlpgpu_lp* lp, int32_t precision, const double* tau
  * is a cudaStream_t (NULL = default stream); the call only enqueues work.
  * Scratch is a fixed 192 KiB static device array inside the library, so rows
  * and columns are limited to 8,388,608 each (larger sizes are rejected with an
- * error). The first call on a device looks up that array's address, so make
- * the first call on each device before any stream capture. All calls share
+ * error), and a NULL pointer that a launch would read or write is rejected
+ * before anything is enqueued. The first call in each CUDA context (the
+ * device's primary context, again after cudaDeviceReset, or a caller's own
+ * driver context) looks up that array's address in that context, so make the
+ * first call in each context before any stream capture. All calls share
  * the array: calls that overlap on the GPU race; each call writes every slot
  * it later reads, so nothing needs clearing between calls. Returns 0, or -1
  * with pdlpgpu_last_error() set. */

@@ -22,6 +22,7 @@
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <vector>
 
 extern "C" void pdlpgpu_internal_set_error(const char* message);
 
@@ -36,9 +37,21 @@ constexpr unsigned kFull = 0xffffffffu;
 // Slots [0, kNaMaxCtas): primal partials; then two per dual CTA.
 static __device__ __align__(256) double g_noalloc_scratch[3 * kNaMaxCtas];
 
-// Address of the array on each device, looked up once per device.
+// Address of the array in each CUDA context it was looked up in. The key is
+// the context's unique ID, not the device ordinal: after cudaDeviceReset, or
+// under a caller's own driver context, the library's module is loaded again at
+// another address, and a lookup made in an earlier context would be stale.
+// Context IDs are never reused within a process, unlike context handles.
+struct ScratchEntry {
+    unsigned long long context_id;
+    double* address;
+};
 std::mutex g_scratch_mutex;
-double* g_scratch_address[64] = {nullptr};
+std::vector<ScratchEntry> g_scratch_entries;
+using CtxGetCurrent = int (*)(void**);                    // cuCtxGetCurrent(CUcontext*)
+using CtxGetId = int (*)(void*, unsigned long long*);     // cuCtxGetId(CUcontext, id*)
+CtxGetCurrent g_ctx_get_current = nullptr;
+CtxGetId g_ctx_get_id = nullptr;
 
 __device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }
 __device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }
@@ -137,31 +150,65 @@ __global__ void na_reduce(int primal_ctas, int dual_ctas, const double* scratch,
     out[2] = it;
 }
 
-// Device address of the scratch array for the current device. The first call
-// on each device does the lookup (with that device current); later calls
+bool driver_entry(const char* name, void** fn, std::string& error) {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint(name, fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || *fn == nullptr) {
+        error = std::string(name) + " unavailable";
+        return false;
+    }
+    return true;
+}
+
+// Device address of the scratch array in the current context. The first call
+// in each context does the lookup (with that context current); later calls
 // reuse it.
-double* scratch_on_current_device(std::string& error) {
-    int device = 0;
-    cudaError_t rc = cudaGetDevice(&device);
-    if (rc != cudaSuccess) {
-        error = std::string("cudaGetDevice: ") + cudaGetErrorString(rc);
-        return nullptr;
-    }
-    if (device < 0 || device >= 64) {
-        error = "device ordinal out of range";
-        return nullptr;
-    }
+double* scratch_in_current_context(std::string& error) {
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (g_scratch_address[device] == nullptr) {
-        double* p = nullptr;
-        rc = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_noalloc_scratch);
+    if (g_ctx_get_current == nullptr || g_ctx_get_id == nullptr) {
+        void* current = nullptr;
+        void* id = nullptr;
+        if (!driver_entry("cuCtxGetCurrent", &current, error) ||
+            !driver_entry("cuCtxGetId", &id, error))
+            return nullptr;
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrent>(current);
+        g_ctx_get_id = reinterpret_cast<CtxGetId>(id);
+    }
+    void* context = nullptr;
+    double* fresh = nullptr;
+    if (g_ctx_get_current(&context) != 0) {
+        error = "cuCtxGetCurrent failed";
+        return nullptr;
+    }
+    if (context == nullptr) {
+        // No context is current yet: the runtime makes the device's primary
+        // context current while it resolves the symbol.
+        const cudaError_t rc = cudaGetSymbolAddress(reinterpret_cast<void**>(&fresh), g_noalloc_scratch);
         if (rc != cudaSuccess) {
             error = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(rc);
             return nullptr;
         }
-        g_scratch_address[device] = p;
+        if (g_ctx_get_current(&context) != 0 || context == nullptr) {
+            error = "no current CUDA context";
+            return nullptr;
+        }
     }
-    return g_scratch_address[device];
+    unsigned long long id = 0;
+    if (g_ctx_get_id(context, &id) != 0) {
+        error = "cuCtxGetId failed";
+        return nullptr;
+    }
+    for (const ScratchEntry& e : g_scratch_entries)
+        if (e.context_id == id) return e.address;
+    if (fresh == nullptr) {
+        const cudaError_t rc = cudaGetSymbolAddress(reinterpret_cast<void**>(&fresh), g_noalloc_scratch);
+        if (rc != cudaSuccess) {
+            error = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(rc);
+            return nullptr;
+        }
+    }
+    g_scratch_entries.push_back({id, fresh});
+    return fresh;
 }
 
 int fail(const std::string& message) {
@@ -185,8 +232,27 @@ extern "C" int32_t pdlpgpu_trial_noalloc(
         return fail("pdlpgpu_trial_noalloc: at most 8388608 rows and 8388608 columns "
                     "(the static scratch holds 8192 partial sums per half)");
     if (!(weight > 0.0)) return fail("pdlpgpu_trial_noalloc: weight must be positive");
+    // Every pointer a launch would dereference must be given: NULL is refused
+    // here, before anything is enqueued, instead of faulting on the device.
+    if (reductions == nullptr) return fail("pdlpgpu_trial_noalloc: reductions is NULL");
+    if (cols > 0) {
+        const void* column_side[] = {at_row_start, at_col_index, at_values, objective, var_lower,
+                                     var_upper, tau, tau_inverse, x, x_out};
+        for (const void* p : column_side)
+            if (p == nullptr)
+                return fail("pdlpgpu_trial_noalloc: a column-side pointer (A^T, objective, "
+                            "variable bounds, tau, x, x_out) is NULL with cols > 0");
+    }
+    if (rows > 0) {
+        const void* row_side[] = {a_row_start, a_col_index, a_values, row_lower, row_upper,
+                                  sigma, sigma_inverse, y, ax, y_out, ax_out};
+        for (const void* p : row_side)
+            if (p == nullptr)
+                return fail("pdlpgpu_trial_noalloc: a row-side pointer (A, row bounds, sigma, "
+                            "y, ax, y_out, ax_out) is NULL with rows > 0");
+    }
     std::string error;
-    double* scratch = scratch_on_current_device(error);
+    double* scratch = scratch_in_current_context(error);
     if (scratch == nullptr) return fail("pdlpgpu_trial_noalloc: " + error);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int pc = static_cast<int>((int64_t(cols) + kNaLinesPerCta - 1) / kNaLinesPerCta);

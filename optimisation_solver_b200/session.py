@@ -31,21 +31,55 @@ def _caller_stream_done():
         current.synchronize()
 
 
-def _check_sizes(arrs, rows, n, m):
+def _check_buffer(a, name, needed, on_device, in_place):
+    """A buffer the library reads or writes as `needed` contiguous doubles.
+    Host inputs are converted to contiguous float64 copies before the call,
+    so only their element count matters; device inputs and every output are
+    used in place (`in_place`), so they must already be contiguous float64
+    storage of at least `needed` elements, on the side the call names. Raw
+    integer device pointers are the caller's responsibility."""
+    if a is None or isinstance(a, int):
+        return
+    if hasattr(a, "data_ptr"):   # a torch tensor
+        if on_device != a.is_cuda:
+            where = "a CUDA" if on_device else "a host"
+            raise ValueError(f"{name}: {where} tensor expected")
+        if in_place:
+            import torch
+            if a.dtype != torch.float64:
+                raise ValueError(f"{name}: dtype {a.dtype}, float64 expected")
+            if not a.is_contiguous():
+                raise ValueError(f"{name}: tensor is not contiguous")
+        size = a.numel()
+    else:
+        if on_device:
+            raise ValueError(f"{name}: a device buffer (CUDA tensor or integer address) expected")
+        if in_place and (not isinstance(a, np.ndarray) or a.dtype != np.float64
+                         or not a.flags.c_contiguous or not a.flags.writeable):
+            raise ValueError(f"{name}: a writeable C-contiguous float64 numpy array expected")
+        size = np.size(a)
+    if size < needed:
+        raise ValueError(f"{name}: {size} elements, at least {needed} expected")
+
+
+def _check_sizes(arrs, rows, n, m, on_device=False):
     """The library reads rows x length elements of each per-instance input
     (objective, row bounds, variable bounds, warm primal, warm dual, warm
-    weight), the first rows of a larger one: an array or tensor with fewer
-    elements is refused here rather than read past its end. Raw integer
-    device pointers are the caller's responsibility."""
+    weight), the first rows of a larger one: a buffer with fewer elements, or
+    device storage of another dtype or with gaps, is refused here rather than
+    read past its end."""
     names = ("objective", "row_lower", "row_upper", "var_lower", "var_upper", "warm_primal",
              "warm_dual", "warm_weight")
     lengths = (n, m, m, n, n, n, m, 1)
     for a, name, k in zip(arrs, names, lengths):
-        if a is None or isinstance(a, int):
-            continue
-        size = a.numel() if hasattr(a, "numel") else np.size(a)
-        if size < rows * k:
-            raise ValueError(f"{name}: {size} elements, at least {rows} x {k} expected")
+        _check_buffer(a, name, rows * k, on_device, in_place=on_device)
+
+
+def _check_output(a, name, needed, on_device):
+    """An output the library writes in place: on the host a writeable
+    C-contiguous float64 numpy array, on the device a contiguous float64 CUDA
+    tensor (or an integer address), of at least `needed` elements."""
+    _check_buffer(a, name, needed, on_device, in_place=True)
 
 
 def _addr(a):
@@ -96,7 +130,7 @@ class Session:
              on_device: bool = False):
         arrs = [objective, row_lower, row_upper, var_lower, var_upper, warm_primal, warm_dual,
                 warm_weight]
-        _check_sizes(arrs, self.batch, self.n, self.m)
+        _check_sizes(arrs, self.batch, self.n, self.m, on_device)
         if not on_device:
             arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
         else:
@@ -115,6 +149,8 @@ class Session:
     def read(self, primal=None, dual=None, on_device: bool = False):
         """Statuses, iterations and stats on the host; primal/dual into the
         given buffers (allocated on the host when None and on_device is False)."""
+        _check_output(primal, "primal", self.batch * self.n, on_device)
+        _check_output(dual, "dual", self.batch * self.m, on_device)
         if not on_device:
             if primal is None:
                 primal = np.zeros((self.batch, self.n))
@@ -144,7 +180,7 @@ class Session:
         writes into the given device buffers (or none)."""
         arrs = [objective, row_lower, row_upper, var_lower, var_upper, warm_primal, warm_dual,
                 warm_weight]
-        _check_sizes(arrs, int(count), self.n, self.m)
+        _check_sizes(arrs, int(count), self.n, self.m, on_device)
         if not on_device:
             arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
             if primal is None:
@@ -153,6 +189,8 @@ class Session:
                 dual = np.zeros((count, self.m))
         else:
             _caller_stream_done()
+        _check_output(primal, "primal", int(count) * self.n, on_device)
+        _check_output(dual, "dual", int(count) * self.m, on_device)
         status = np.zeros(count, dtype=np.int32)
         iters = np.zeros(count, dtype=np.int64)
         stats = np.zeros((count, 8))

@@ -1,5 +1,6 @@
 """The C-ABI library loads on a host without a GPU and exports every symbol
 the public headers declare; host-only entry points work without a device."""
+import ctypes as C
 import os
 import re
 
@@ -102,3 +103,57 @@ def test_session_refuses_short_inputs_before_any_device_work():
         _check_sizes([None, np.zeros((3, m))] + [None] * 6, 4, n, m)
     with pytest.raises(ValueError, match="warm_weight"):
         _check_sizes([None] * 7 + [np.zeros(3)], 4, n, m)
+
+
+def test_session_refuses_mistyped_and_short_buffers():
+    """Buffers the library uses in place (device inputs, every output) must be
+    contiguous float64 storage of at least the size it reads or writes; host
+    memory passed as a device buffer is refused too. All checked before any
+    C call, so this runs without a GPU."""
+    import pytest
+    import torch
+
+    from optimisation_solver_b200.session import _check_output, _check_sizes
+    n, m = 5, 3
+    _check_output(np.zeros((4, n)), "primal", 4 * n, False)
+    with pytest.raises(ValueError, match="float64"):
+        _check_output(np.zeros((4, n), np.float32), "primal", 4 * n, False)
+    with pytest.raises(ValueError, match="at least 20"):
+        _check_output(np.zeros((3, n)), "primal", 4 * n, False)
+    with pytest.raises(ValueError, match="C-contiguous"):
+        _check_output(np.zeros((n, 8))[:, :4].T, "primal", 4 * n, False)
+    with pytest.raises(ValueError, match="float64"):
+        _check_output(torch.zeros(4 * n, dtype=torch.float32), "primal", 4 * n, False)
+    # host memory where the call expects device memory
+    with pytest.raises(ValueError, match="device buffer"):
+        _check_sizes([np.zeros((4, n))] + [None] * 7, 4, n, m, on_device=True)
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        _check_sizes([torch.zeros(4 * n, dtype=torch.float64)] + [None] * 7, 4, n, m,
+                     on_device=True)
+    # host inputs are copied to float64, so their dtype does not matter
+    _check_sizes([np.zeros((4, n), np.float32)] + [None] * 7, 4, n, m)
+
+
+def test_noalloc_trial_rejects_null_pointers_before_any_launch():
+    """pdlpgpu_trial_noalloc refuses NULL device pointers on the side that has
+    lines (and a NULL reductions pointer) with -1 before it touches a device,
+    so this runs on a host without a GPU."""
+    lib = native.lib()
+    one = (C.c_double * 4)()
+    fake = C.cast(one, C.c_void_p)   # never dereferenced: the call fails first
+    # reductions NULL
+    rc = lib.pdlpgpu_trial_noalloc(2, 3, *([fake] * 18), 1.0, 1.0, fake, fake, fake, None, None)
+    assert rc == -1 and "reductions is NULL" in native.last_error()
+    # a column-side pointer NULL with columns present (the objective, argument 9)
+    args = [fake] * 18
+    args[6] = None
+    rc = lib.pdlpgpu_trial_noalloc(2, 3, *args, 1.0, 1.0, fake, fake, fake, fake, None)
+    assert rc == -1 and "column-side" in native.last_error()
+    # a row-side pointer NULL with rows present (y)
+    args = [fake] * 18
+    args[16] = None
+    rc = lib.pdlpgpu_trial_noalloc(2, 3, *args, 1.0, 1.0, fake, fake, fake, fake, None)
+    assert rc == -1 and "row-side" in native.last_error()
+    # x_out NULL with columns present
+    rc = lib.pdlpgpu_trial_noalloc(2, 3, *([fake] * 18), 1.0, 1.0, None, fake, fake, fake, None)
+    assert rc == -1 and "column-side" in native.last_error()
