@@ -1,0 +1,160 @@
+"""The batched paths pinned directly to the CPU oracle (the reference
+pdlp_engine built from its sources), not through the engine's own one-LP
+solves:
+
+* the headline path -- a stream of flow-family instances through a
+  mixed-precision session in the batch-interleaved layout -- at 1e-4: same
+  status as the reference, every returned point rescored by the reference's
+  TerminationChecker within 1e-4, the device's FP64 scores equal to the
+  reference's, objectives within the gap bound;
+* FP64 sessions at 1e-8: objectives within 1e-6 relative of the reference's
+  (the FP64-mode bar);
+* `solve_batch` of planted LPs of uneven sizes, FP64 and mixed;
+* small shapes of the single-LP configurations: the Zipf-degree, log-uniform
+  magnitude family of the large LP, and its rescaled, free-variable,
+  ranged-row stress variant;
+* the power iteration (diagonal preconditioning off): the static step bound
+  from `Preconditioner::estimateSpectralNorm` (pdlp_engine/src/preconditioner.cpp:82-140).
+
+Acceptance rules: tests/parity.py.
+"""
+import numpy as np
+import pytest
+
+from optimisation_solver_b200 import generators as g
+from optimisation_solver_b200.lp import PdlpOptions, PdlpStatus
+from optimisation_solver_b200.pdlp import PdlpSolver
+from optimisation_solver_b200.session import Session
+from tests import cases
+from tests.parity import check_objective, check_point, solve_many
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def flow():
+    G = g.flow_graph()
+    s, c = g.flow_parameters(G, 64, seed=901)
+    return G, s, c
+
+
+def _scores(out, i):
+    return {k: out[k][i] for k in ("primal_residual", "dual_residual", "relative_gap",
+                                   "primal_objective", "dual_objective")}
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_flow_stream_interleaved_matches_oracle_at_1e4(oracle, flow, precision):
+    """64 instances through 32 slots (every slot refilled once), cold start."""
+    G, s, c = flow
+    tol = 1e-4
+    family = g.flow_lp(G, s[0], c[0])
+    S = Session(family, 32, PdlpOptions().with_tolerance(tol), precision=precision,
+                layout="interleaved")
+    out = S.stream(64, objective=c, row_lower=s, row_upper=s)
+    S.close()
+    lps = [g.flow_lp(G, s[i], c[i]) for i in range(64)]
+    refs = solve_many(oracle, lps, tol)
+    for i, (lp, ref) in enumerate(zip(lps, refs)):
+        assert str(out["status"][i]) == ref.status == "optimal", (i, out["status"][i], ref.status)
+        check_point(oracle, lp, out["primal"][i], out["dual"][i], tol, _scores(out, i))
+        check_objective(out["primal_objective"][i], ref, tol)
+
+
+def test_flow_session_fp64_matches_oracle_objective_at_1e8(oracle, flow):
+    """FP64 mode: objectives within 1e-6 relative of the reference's, both
+    solved to 1e-8."""
+    G, s, c = flow
+    tol, count = 1e-8, 16
+    family = g.flow_lp(G, s[0], c[0])
+    S = Session(family, count, PdlpOptions().with_tolerance(tol), precision="fp64",
+                layout="interleaved")
+    S.load(objective=c[:count], row_lower=s[:count], row_upper=s[:count])
+    S.solve()
+    out = S.read()
+    S.close()
+    lps = [g.flow_lp(G, s[i], c[i]) for i in range(count)]
+    refs = solve_many(oracle, lps, tol)
+    for i, (lp, ref) in enumerate(zip(lps, refs)):
+        assert str(out["status"][i]) == ref.status == "optimal"
+        check_point(oracle, lp, out["primal"][i], out["dual"][i], tol, _scores(out, i))
+        check_objective(out["primal_objective"][i], ref, tol, objective_rel=1e-6)
+
+
+def _uneven_planted(count=12, lo=200, hi=3000, seed=5):
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), count)).astype(int)
+    out = []
+    for i, m in enumerate(sizes):
+        deg = np.random.default_rng(700 + i).integers(4, 13, size=2 * int(m))
+        out.append(g.planted_lp(int(m), 2 * int(m), seed=100 + i, degrees=deg))
+    return out
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-8), ("mixed", 1e-4)])
+def test_solve_batch_uneven_planted_matches_oracle(oracle, precision, tol):
+    planted = _uneven_planted()
+    lps = [p.lp for p in planted]
+    results = PdlpSolver(precision).solve_batch(lps, PdlpOptions().with_tolerance(tol))
+    refs = solve_many(oracle, lps, tol)
+    for lp, r, ref in zip(lps, results, refs):
+        assert str(r.status) == ref.status == "optimal", (r.status, ref.status)
+        scores = dict(primal_residual=r.primal_residual, dual_residual=r.dual_residual,
+                      relative_gap=r.relative_gap, primal_objective=r.primal_objective,
+                      dual_objective=r.dual_objective)
+        check_point(oracle, lp, r.primal, r.row_dual, tol, scores)
+        if precision == "fp64":
+            check_objective(r.primal_objective, ref, tol, objective_rel=1e-6)
+        else:
+            check_objective(r.primal_objective, ref, tol)
+
+
+SHAPES = [
+    # Zipf column degrees, log-uniform magnitudes, 30% equality rows, box bounds.
+    ("large_3k", lambda: g.large_lp(0, m=3000, n=6000)),
+    # The same rescaled by factors in [1e-4, 1e4], 20% free variables, 10% ranged rows.
+    ("stress_3k", lambda: g.stress_lp(0, m=3000, n=6000)),
+]
+
+
+@pytest.mark.parametrize("name,build", SHAPES, ids=[s[0] for s in SHAPES])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_single_lp_shapes_match_reference_at_1e4(oracle, name, build, precision):
+    """Both solvers stop on the reference's relative criteria. On the stress
+    family those pass well away from the planted optimum (the reference also
+    stops 0.4% off it at this size and 18% off at 8000 rows), so the objective
+    is compared with the reference's own, within the gap bound, and the point
+    is rescored by the reference."""
+    tol = 1e-4
+    p = build()
+    opts = PdlpOptions().with_tolerance(tol)
+    opts.iteration_limit = 400000
+    r = PdlpSolver(precision).solve(p.lp, opts)
+    (ref,) = solve_many(oracle, [p.lp], tol, iteration_limit=400000)
+    assert str(r.status) == ref.status == "optimal", (r.status, ref.status)
+    check_point(oracle, p.lp, r.primal, r.row_dual, tol)
+    check_objective(r.primal_objective, ref, tol)
+
+
+POWER_CASES = [
+    ("planted_1000x2000", lambda: g.reference_lp(0).lp),
+    ("random_feasible", lambda: cases.random_feasible(300, 420, 21)),
+    ("feasible_box", lambda: cases.feasible_box(2500, 3000, 5, per_row=10)),
+]
+
+
+@pytest.mark.parametrize("name,build", POWER_CASES, ids=[c[0] for c in POWER_CASES])
+def test_power_iteration_matches_oracle(oracle, name, build):
+    """Diagonal preconditioning off: the step bound comes from the power
+    iteration on A'A (mt19937 seed 1), run on the device in FP64."""
+    lp = build()
+    opts = PdlpOptions().with_tolerance(1e-8)
+    opts.use_diagonal_preconditioning = False
+    r = PdlpSolver("fp64").solve(lp, opts)
+    (ref,) = solve_many(oracle, [lp], 1e-8, use_diagonal_preconditioning=0)
+    assert r.static_step_bound > 0.0
+    assert abs(r.static_step_bound - ref.static_step_bound) <= 1e-9 * ref.static_step_bound, (
+        r.static_step_bound, ref.static_step_bound)
+    assert str(r.status) == ref.status
+    if ref.status == "optimal":
+        check_objective(r.primal_objective, ref, 1e-8, objective_rel=1e-6)

@@ -1,0 +1,94 @@
+"""The GPU engine behind the reference's own pipeline (end to end).
+
+`oracle/Makefile` links the reference's presolve, dispatch, engines and
+postsolve with the GPU engine's pdlp::PdlpSolver::solve
+(include/pdlpgpu_override.hpp) in place of pdlp_engine/src/pdlp_solver.cpp,
+so solver::runPdlp (src/solver/orchestrator.cpp:315-352) calls the GPU with no
+reference line changed. Checked here:
+
+* the reference's own pipeline test, tests/pipeline/test_postsolve_integration.cpp,
+  every case (forced PDLP: x = {2, 0, 5.6}, objective 39.4, duals {0, 0.8, 0},
+  reduced costs {5, -0.2, 0}; limit semantics; failure statuses);
+* the reference's LP fixture files (benchmarks/instances/known/*.mps and
+  netlib/afiro.mps, carried as Model IR arrays in tests/golden/) through
+  solver::solve with PDLP forced: their published objectives to 1e-6
+  relative, the statuses of the infeasible and unbounded files, and the
+  reference pipeline's own primal values, shadow prices and reduced costs;
+* the same fixtures compiled by adapter::toCompiledLp and solved by the engine
+  directly, against the reference oracle on the same CompiledLp;
+* the 1000 x 2000 planted LP written as free-format MPS, read back by the
+  reference MpsReader and solved through the pipeline.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from optimisation_solver_b200 import generators as g
+from optimisation_solver_b200.lp import PdlpOptions
+from optimisation_solver_b200.pdlp import PdlpSolver
+from oracle.pipeline import ENGINE_PDLP, POSTSOLVE_TEST, Pipeline, available
+from tests.mps_writer import write_free_mps
+from tests.parity import check_objective, solve_many
+from tests.test_pipeline import fixture_models
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not available("gpu"),
+                                 reason="GPU pipeline not built (make -C oracle pipeline)")]
+
+CASES = ["lp_engines", "qp_signs", "all_eliminated", "bound_only", "integer_models",
+         "unavailable_duals", "failure_statuses", "limit_no_solution", "limit_feasible_solution",
+         "reduced_api"]
+
+
+@pytest.fixture(scope="module")
+def gpu_pipeline():
+    return Pipeline("gpu")
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_reference_postsolve_integration_with_gpu_engine(case):
+    r = subprocess.run([POSTSOLVE_TEST["gpu"], case], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and f"[PASSED] {case}" in r.stdout, r.stdout + r.stderr
+
+
+def test_fixture_files_through_gpu_pipeline(gpu_pipeline):
+    for name, d in fixture_models().items():
+        r = gpu_pipeline.import_model(d).solve(engine=ENGINE_PDLP, tolerance=1e-8)
+        assert r.status == str(d["pdlp_status"]), (name, r.status, r.message)
+        if r.status != "optimal":
+            continue
+        assert r.executed_engine == ENGINE_PDLP, name
+        want = float(d["expected_objective"])
+        assert abs(r.objective - want) <= 1e-6 * max(1.0, abs(want)), (name, r.objective, want)
+        # The reference pipeline's own PDLP answer (both at 1e-8).
+        for field in ("x", "duals", "reduced_costs"):
+            got, ref = getattr(r, field), d[f"pdlp_{field}"]
+            assert got.shape == ref.shape, (name, field)
+            assert np.allclose(got, ref, rtol=1e-5, atol=1e-5), (name, field, got, ref)
+
+
+def test_compiled_fixtures_engine_matches_oracle(oracle, gpu_pipeline):
+    lps, names = [], []
+    for name, d in fixture_models().items():
+        lps.append(gpu_pipeline.import_model(d).compile())
+        names.append(name)
+    refs = solve_many(oracle, lps, 1e-8)
+    solver = PdlpSolver("fp64")
+    for name, lp, ref in zip(names, lps, refs):
+        r = solver.solve(lp, PdlpOptions().with_tolerance(1e-8))
+        assert str(r.status) == ref.status, (name, r.status, ref.status)
+        if ref.status == "optimal":
+            check_objective(r.primal_objective, ref, 1e-8, objective_rel=1e-6)
+
+
+def test_planted_lp_mps_file_through_gpu_pipeline(tmp_path, gpu_pipeline):
+    planted = g.reference_lp(0)
+    path = str(tmp_path / "planted_0.mps")
+    write_free_mps(planted.lp, path, "planted_0")
+    model = gpu_pipeline.read_mps(path)
+    r = model.solve(engine=ENGINE_PDLP, tolerance=1e-8)
+    assert r.status == "optimal" and r.executed_engine == ENGINE_PDLP, r.message
+    assert abs(r.objective - planted.objective) <= 1e-6 * abs(planted.objective)
+    assert r.has_duals and r.max_dual_residual < 1e-5
