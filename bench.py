@@ -152,6 +152,31 @@ def workload(batch: int, steps: int, rank: int, graph):
     return [g.flow_parameters(graph, batch, seed=sd) for sd in rank_seeds(rank, steps)]
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_solve_sequential(lib_kind: str, graph, supply, cost, tol: float, threads: int):
+    """The instances one after another, each solve with `threads` solver
+    threads (the reference parallelises one LP above 20,000 nonzeros). Returns
+    (seconds, statuses)."""
+    from oracle.oracle import Oracle
+    from optimisation_solver_b200 import generators as g
+    orc = Oracle(lib_kind)
+    opts = dict(thread_count=threads, primal_tolerance=tol, dual_tolerance=tol, gap_tolerance=tol)
+    lps = [g.flow_lp(graph, supply[i], cost[i]) for i in range(supply.shape[0])]
+    t0 = time.perf_counter()
+    res = [orc.solve(lp, opts) for lp in lps]
+    return time.perf_counter() - t0, [r.status for r in res]
+
+
 def cpu_solve_sample(lib_kind: str, graph, supply, cost, tol: float, threads: int):
     """Solves each (supply, cost) instance with the CPU library, instance
     parallel over `threads` host threads (one solver thread each). Returns
@@ -182,9 +207,27 @@ def trial_bytes(n, m, nnz, slots, s, family_bounds_x=True):
     return primal, dual
 
 
+def launch_ranks(args) -> int:
+    """`--gpus N` outside torchrun: start N ranks on this node with the same
+    arguments (one process per GPU, rendezvous on 127.0.0.1) and return the
+    launcher's exit status. Rank 0 prints the JSON line."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+           os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
+
+
 def main():
     args = parse_args()
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        sys.exit(launch_ranks(args))
     world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}: launch one rank per GPU")
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     assert args.warmup >= 3, "at least 3 warm-up steps"
@@ -271,13 +314,14 @@ def main():
             launches += 2 + model.mlp.launches()
         return wx, wy, ww, launches
 
-    def solve(sup, cost, outx=None, outy=None, warm=True):
+    def solve(sup, cost, outx=None, outy=None, warm=True, sess=None):
+        sess = session if sess is None else sess
         wx, wy, ww, launches = predict(sup, cost) if warm else (None, None, None, 0)
         ptr = lambda t: None if t is None else t.data_ptr()
-        res = session.stream(sup.shape[0], objective=ptr(cost), row_lower=ptr(sup), row_upper=ptr(sup),
+        res = sess.stream(sup.shape[0], objective=ptr(cost), row_lower=ptr(sup), row_upper=ptr(sup),
                              warm_primal=ptr(wx), warm_dual=ptr(wy), warm_weight=ptr(ww),
                              primal=ptr(outx), dual=ptr(outy), on_device=True)
-        return res, launches + session.last_timing()[1]
+        return res, launches + sess.last_timing()[1]
 
     # Warm-up: the first W steps, each solved on its own.
     for k in range(W):
@@ -362,7 +406,7 @@ def main():
 
     if rank == 0 and not args.no_extras:
         line["extras"] = extras(args, session, graph, sup_all[timed], cost_all[timed], steps_in[-1],
-                                value, iters, solve)
+                                value, iters, solve, family, options, local_rank)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, graph, steps_in[-1], res)
     session.close()
@@ -471,12 +515,30 @@ def side_workload(args, rank: int, world: int, local_rank: int):
     return line
 
 
-def extras(args, session, graph, sup, cost, inputs, value, iters, solve):
-    """Side measurements: the same instances cold (the learned gain), plain
-    FP64 one-LP-per-call GPU PDLP (the comparison the target is quoted
-    against), and the trial kernels on the single large LP."""
+def extras(args, session, graph, sup, cost, inputs, value, iters, solve, family, options, device):
+    """Side measurements: the same instances cold (the learned gain), the same
+    instances with FP64 iterations (the share of the speed-up that FP32
+    arithmetic brings), plain FP64 one-LP-per-call GPU PDLP (the comparison
+    the target is quoted against), and the trial kernels on the single large
+    LP."""
     import torch
+
+    from optimisation_solver_b200.session import Session
     out = {}
+    if args.precision == "mixed":
+        s64 = Session(family, args.slots, options, precision="fp64", device=device)
+        solve(sup[: args.batch], cost[: args.batch], warm=not args.cold, sess=s64)   # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r64, _ = solve(sup, cost, warm=not args.cold, sess=s64)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        s64.close()
+        out["fp64_batched"] = {"lps_per_s": round(sup.shape[0] / dt, 2),
+                               "mean_iterations": float(r64["iterations"].mean()),
+                               "optimal_fraction": r64["optimal"] / sup.shape[0],
+                               "warm_start": "cold" if args.cold else "learned",
+                               "mixed_over_fp64": round(value / (sup.shape[0] / dt), 3)}
     if not args.cold:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -495,8 +557,10 @@ def extras(args, session, graph, sup, cost, inputs, value, iters, solve):
     return out
 
 
-def plain_gpu(graph, inputs, tol, count=6):
-    """Plain FP64 single-instance GPU PDLP on the same instances, one LP per call."""
+def plain_gpu(graph, inputs, tol, count=32):
+    """Plain FP64 single-instance GPU PDLP on the same instances, one LP per
+    call; the device time of the solves and the host time around them are
+    reported apart."""
     from optimisation_solver_b200 import generators as g
     from optimisation_solver_b200.lp import PdlpOptions
     from optimisation_solver_b200.pdlp import PdlpSolver
@@ -507,12 +571,17 @@ def plain_gpu(graph, inputs, tol, count=6):
     # The LPs are built before the clock starts: only the solves are timed.
     lps = [g.flow_lp(graph, supply[i], cost[i]) for i in range(1, count + 1)]
     t0 = time.perf_counter()
-    iters = []
+    iters, device = [], 0.0
     for lp in lps:
         r = solver.solve(lp, opts)
         iters.append(r.iterations)
+        device += r.device_seconds
     dt = time.perf_counter() - t0
-    return {"lps_per_s": round(count / dt, 3), "instances": count, "mean_iterations": float(np.mean(iters))}
+    return {"lps_per_s": round(count / dt, 3), "instances": count,
+            "mean_iterations": float(np.mean(iters)),
+            "device_seconds_per_lp": round(device / count, 5),
+            "host_seconds_per_lp": round((dt - device) / count, 5),
+            "us_per_iteration": round(1e6 * device / max(1, sum(iters)), 2)}
 
 
 def large_lp_kernels():
@@ -547,11 +616,19 @@ def cpu_baseline(args, graph, inputs, res):
     seconds, statuses, objs = cpu_solve_sample(kind, graph, supply[:k], cost[:k], args.tol, threads)
     last = res["primal_objective"][-args.batch:][:k]
     rel = np.abs(last - np.array(objs)) / (1.0 + np.abs(np.array(objs)))
+    ks = min(8, k)
+    seq_seconds, seq_statuses = cpu_solve_sequential(kind, graph, supply[:ks], cost[:ks], args.tol,
+                                                     threads)
     return {"value": round(k / seconds, 3), "unit": "LPs/s", "cores": threads,
+            "cpu_model": cpu_model(),
             "kind": "reference" if kind == "ref_fast" else "port",
             "sample": f"{k} instances of the last step, instance-parallel, one solver thread each, "
                       f"{seconds:.1f} s",
             "optimal_fraction": statuses.count("optimal") / k,
+            "sequential_all_cores": {"value": round(ks / seq_seconds, 3), "unit": "LPs/s",
+                                     "sample": f"{ks} instances one after another, {threads} solver "
+                                               f"threads each, {seq_seconds:.1f} s",
+                                     "optimal_fraction": seq_statuses.count("optimal") / ks},
             "device_vs_cpu_objective_rel_max": float(rel.max())}
 
 
@@ -583,6 +660,7 @@ def reference_arm(args, world, rank, graph, config):
             "config": dict(config, batch=per_step, warm_start="cold (the reference has no warm start)"),
             "impl": "reference", "optimal_fraction": optimal / (per_step * args.steps),
             "cpu_baseline": {"value": round(value, 3), "unit": "LPs/s", "cores": threads,
+                             "cpu_model": cpu_model(),
                              "kind": "reference" if kind == "ref_fast" else "port",
                              "sample": f"{per_step} instances per step, instance-parallel"},
             "e2e": {"value": round(value, 3), "unit": "LPs/s", "h2d_bytes_per_step": 0,

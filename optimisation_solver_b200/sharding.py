@@ -67,3 +67,22 @@ def weak_scaling_rate(per_rank_units: float, per_rank_seconds: float, device=Non
     units = sum_over_ranks(per_rank_units, device)
     seconds = max_over_ranks(per_rank_seconds, device)
     return units / seconds if seconds > 0 else float("nan")
+
+
+def gather_to_rank0(indices, records):
+    """Per-instance records of every rank's shard, assembled in instance
+    order on rank 0 (None on the other ranks). `indices` are the rank's
+    instance indices, `records` one picklable summary per instance (status,
+    objective, iterations -- small; solutions stay on their rank). Without
+    torch.distributed the records are returned as they are."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return list(records)
+    world = dist.get_world_size()
+    mine = list(zip([int(i) for i in indices], records))
+    parts = [None] * world if dist.get_rank() == 0 else None
+    dist.gather_object(mine, parts, dst=0)
+    if dist.get_rank() != 0:
+        return None
+    pairs = sorted((p for part in parts for p in part), key=lambda t: t[0])
+    return [r for _, r in pairs]
