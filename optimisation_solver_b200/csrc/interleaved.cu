@@ -26,21 +26,20 @@ constexpr int kIlWarps = 8;
 constexpr int kIlThreads = kIlWarps * 32;
 
 // True in every thread of the CTA that arrives last of `expected` CTAs
-// (and resets the counter). Everything written before is visible to it.
-// One thread fences for the CTA: the barrier orders the other threads'
-// writes before its fence, and a fence covers the writes its thread has
-// observed (the pattern of a cooperative grid barrier).
+// (and resets the counter; the next use is in a later kernel). Everything
+// written before is visible to it. One thread arrives for the CTA with an
+// acquire-release atomic at GPU scope: the barrier orders the other
+// threads' writes before it, its release publishes them, and in the last CTA
+// its acquire makes every earlier arrival's writes visible -- one round trip
+// where a full fence and an atomic took two.
 __device__ __forceinline__ bool arrive_last_cta(int32_t* counter, int expected) {
     __shared__ int last;
     __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
-        const int prev = atomicAdd(counter, 1);
+        int prev;
+        asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(prev) : "l"(counter) : "memory");
         last = prev == expected - 1;
-        if (last) {
-            *counter = 0;
-            __threadfence();
-        }
+        if (last) *counter = 0;
     }
     __syncthreads();
     return last != 0;
@@ -54,6 +53,25 @@ __device__ __forceinline__ bool arrive_last_cta(int32_t* counter, int expected) 
 // ahead of a still-running decision two kernels back.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Non-binding bulk prefetch of `bytes` (a multiple of 16, from a 16-byte
+// aligned address) into L2: DRAM bytes in flight that cost no registers.
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Prefetches the group's slice of `kinds` [line][bp] streams for lines
+// [l0, l1): one G-element row (128-512 bytes, 16-byte aligned because bp and
+// the group offset are multiples of G = 32 V) per line and stream.
+template <class T, int kMax>
+__device__ __forceinline__ void prefetch_rows(const T* const (&streams)[kMax], int kinds, int64_t bp,
+                                              int64_t group_off, unsigned row_bytes, int l0, int l1) {
+    const int total = (l1 - l0) * kinds;
+    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+        const int l = l0 + q / kinds, k = q - (q / kinds) * kinds;
+        prefetch_l2(streams[k] + static_cast<int64_t>(l) * bp + group_off, row_bytes);
+    }
+}
 
 // V consecutive elements (one 4/8/16-byte access).
 template <class T, int V>
@@ -540,6 +558,19 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_primal(Interleaved<T> il, 
         const IlTile first = il.at_tiles[t0];
         if (first.staged) stage_tile_async(first, il.at_ptr, il.at_idx, il.at_val, st[0]);
     }
+    // The streams this CTA reads -- the committed x (buffer R, written by the
+    // previous primal kernel), the iterate average and the objective -- were
+    // final before this kernel started (the previous dual kernel waited for
+    // the previous primal kernel to complete), so their first two tiles are
+    // prefetched into L2 before the wait; each tile prefetches the one after.
+    const T* const pstreams[3] = {il.X[R], il.avg_x, il.vec[kIlC]};
+    const int pkinds = ((il.family >> kIlC) & 1) ? 2 : 3;
+    const int64_t goff = static_cast<int64_t>(group) * G;
+    const unsigned rbytes = static_cast<unsigned>(G * sizeof(T));
+    for (int ti = t0; ti < t1 && ti < t0 + 2; ++ti) {
+        const IlTile pt = il.at_tiles[ti];
+        prefetch_rows<T, 3>(pstreams, pkinds, il.bp, goff, rbytes, pt.line0, pt.line0 + pt.lines);
+    }
     pdl_wait();
     pdl_trigger();
     x.ls = lane_state<T, V>(il, ctl, static_cast<int>(x.col0), measure, R, true, hot);
@@ -568,6 +599,10 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_primal(Interleaved<T> il, 
         if (ti + 1 < t1) {
             const IlTile nt = il.at_tiles[ti + 1];
             if (nt.staged) stage_tile_async(nt, il.at_ptr, il.at_idx, il.at_val, st[(ti + 1 - t0) & 1]);
+        }
+        if (ti + 2 < t1) {
+            const IlTile pt = il.at_tiles[ti + 2];
+            prefetch_rows<T, 3>(pstreams, pkinds, il.bp, goff, rbytes, pt.line0, pt.line0 + pt.lines);
         }
         if (t.staged) primal_tile<kPrimalU<T, V>, true, kFam>(x, t, st[(ti - t0) & 1], moved[0]);
         else primal_tile<1, false, kFam>(x, t, st[0], moved[0]);
@@ -758,6 +793,16 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_dual(Interleaved<T> il, In
     if (!__syncthreads_or(x.ls.active != 0)) return;
     const int t0 = il.a_cta[blockIdx.x], t1 = il.a_cta[blockIdx.x + 1];
     if (t0 < t1 && il.a_tiles[t0].staged) stage_row_tile(il, il.a_tiles[t0], st);
+    // Ax and y (buffer R, written by the previous dual kernel, which is
+    // complete) and the dual average: the CTA's rows are prefetched into L2
+    // while the primal kernel finishes.
+    if (t0 < t1) {
+        const T* const dstreams[3] = {il.AX[R], il.Y[R], il.avg_y};
+        const IlTile last = il.a_tiles[t1 - 1];
+        prefetch_rows<T, 3>(dstreams, 3, il.bp, static_cast<int64_t>(group) * G,
+                            static_cast<unsigned>(G * sizeof(T)), il.a_tiles[t0].line0,
+                            last.line0 + last.lines);
+    }
     pdl_wait();
     pdl_trigger();
     x.xt = il.X[W] + x.col0;
@@ -821,7 +866,15 @@ __global__ void __launch_bounds__(kIlThreads, 3) k_il_dual(Interleaved<T> il, In
     const int b = static_cast<int>(gp * G) + t;
     const bool mine = t < G && b < il.count;
     HotCtl h{};
-    if (mine) h = load_hot(ctl + b);
+    if (mine) {
+        // The decision reads fields from every 128-byte line of the block:
+        // they come into L1 while the sums below are fetched.
+        const char* cb = reinterpret_cast<const char*>(ctl + b);
+#pragma unroll
+        for (int q = 128; q < static_cast<int>(sizeof(InstanceCtl)); q += 128)
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(cb + q));
+        h = load_hot(ctl + b);
+    }
     double dd[2] = {0.0, 0.0};
     if (t < G) {
         sum_batches<2, G>(il.part2_dual + gp * il.row_batches * 2 * G, il.row_batches, t, dd);

@@ -183,22 +183,58 @@ __device__ __forceinline__ double warp_range_sum(const double* part, int begin, 
     return t;
 }
 
+// Warp-0 deterministic sums of three ranges of per-CTA partials at once:
+// every lane issues its loads of all three before the first add, so the
+// three reductions cost one round trip instead of three. Each result equals
+// warp_range_sum's for the same range (same per-lane order, same butterfly).
+__device__ __forceinline__ void warp_range_sums3(const double* p0, int b0, int e0, int s0, int q0,
+                                                 const double* p1, int b1, int e1, int s1, int q1,
+                                                 const double* p2, int b2, int e2, int s2, int q2,
+                                                 double (&out)[3]) {
+    const int lane = threadIdx.x & 31;
+    double t[3] = {0.0, 0.0, 0.0};
+    constexpr int kAhead = 4;   // partials per lane and range loaded at once
+    for (int k = 0;; k += 32 * kAhead) {
+        if (b0 + k >= e0 && b1 + k >= e1 && b2 + k >= e2) break;
+        double v[3][kAhead];
+#pragma unroll
+        for (int u = 0; u < kAhead; ++u) {
+            const int o = k + 32 * u + lane;
+            v[0][u] = b0 + o < e0 ? p0[static_cast<int64_t>(b0 + o) * s0 + q0] : 0.0;
+            v[1][u] = b1 + o < e1 ? p1[static_cast<int64_t>(b1 + o) * s1 + q1] : 0.0;
+            v[2][u] = b2 + o < e2 ? p2[static_cast<int64_t>(b2 + o) * s2 + q2] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < kAhead; ++u) {
+            const int o = k + 32 * u + lane;
+            if (b0 + o < e0) t[0] += v[0][u];
+            if (b1 + o < e1) t[1] += v[1][u];
+            if (b2 + o < e2) t[2] += v[2][u];
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        for (int o = 16; o > 0; o >>= 1) t[q] += __shfl_xor_sync(kFull, t[q], o);
+        out[q] = t[q];
+    }
+}
+
 // Arrival counter: returns true in every thread of the CTA that arrives last
 // among `expected` CTAs of the instance (and resets the counter for the next
-// launch). Partials written before the call are visible to that CTA. One
-// thread fences for the CTA: the barrier orders the other threads' writes
-// before its fence, which covers the writes its thread has observed.
+// launch, which a kernel boundary orders). Partials written before the call
+// are visible to that CTA. One thread arrives for the CTA with an
+// acquire-release atomic at GPU scope: the barrier orders the other threads'
+// writes before it, its release publishes them, and in the last CTA its
+// acquire makes every earlier arrival's writes visible -- one round trip
+// where a full fence and an atomic took two.
 __device__ __forceinline__ bool arrive_last(int32_t* counter, int expected) {
     __shared__ int last;
     __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
-        const int prev = atomicAdd(counter, 1);
+        int prev;
+        asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(prev) : "l"(counter) : "memory");
         last = prev == expected - 1;
-        if (last) {
-            *counter = 0;
-            __threadfence();
-        }
+        if (last) *counter = 0;
     }
     __syncthreads();
     return last != 0;
@@ -346,6 +382,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_dual(Global g, Work<T> w, Devic
         g.part_dual[2 * blockIdx.x + 1] = red[1];
     }
     if (g.measure) return;
+    // Whichever CTA turns out last decides: each brings the instance's
+    // control block into its L1 while the arrival is in flight, so the
+    // decision's reads of it do not each wait on L2.
+    if (threadIdx.x < sizeof(InstanceCtl) / 128)
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(reinterpret_cast<const char*>(&c) + 128 * threadIdx.x));
     if (!arrive_last(g.count_dual + cw.instance, inf.a_cta_end - inf.a_cta_begin)) return;
     // Options by reference from shared memory (a reference to the kernel
     // parameter would copy it to local memory in every thread).
@@ -353,10 +394,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_dual(Global g, Work<T> w, Devic
     if (threadIdx.x == 0) so = o;
     __syncthreads();
     if (threadIdx.x < 32) {
-        const double pm = warp_range_sum(g.part_primal, inf.at_cta_begin, inf.at_cta_end, 1, 0);
-        const double dmv = warp_range_sum(g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 0);
-        const double it = warp_range_sum(g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 1);
-        if (threadIdx.x == 0) trial_control(c, so, pm, dmv, it, inf.n);
+        double sums[3];
+        warp_range_sums3(g.part_primal, inf.at_cta_begin, inf.at_cta_end, 1, 0,
+                         g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 0,
+                         g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 1, sums);
+        if (threadIdx.x == 0) trial_control(c, so, sums[0], sums[1], sums[2], inf.n);
     }
 }
 
