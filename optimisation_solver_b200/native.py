@@ -1,4 +1,4 @@
-"""ctypes binding of libpdlpgpu (include/pdlpgpu.h, include/pdlpgpu_components.h).
+"""ctypes binding of libpdlpgpu (include/pdlpgpu*.h).
 
 The library is the product: there is no Python or CPU fallback. If it is not
 built, loading raises ``NativeLibraryMissing`` naming the build command.
@@ -138,6 +138,15 @@ SIGNATURES = {
                                              C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_float, C.c_float, C.c_void_p, C.c_void_p,
                                              C.c_void_p]),
+    # MPS files (include/pdlpgpu_mps.h)
+    "pdlpgpu_mps_read": (C.c_int32, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "pdlpgpu_mps_free": (None, [C.c_void_p]),
+    "pdlpgpu_mps_sizes": (None, [C.c_void_p, _i64p]),
+    "pdlpgpu_mps_name": (C.c_char_p, [C.c_void_p, C.c_int32, C.c_int64]),
+    "pdlpgpu_mps_model": (None, [C.c_void_p, _dp, _i32p, _dp, _i32p, _dp, _dp, _dp, _dp, _i64p,
+                                 _i32p, _dp, _i32p, _i32p, _dp]),
+    "pdlpgpu_mps_lp": (C.c_int32, [C.c_void_p, C.POINTER(Lp), _i32p]),
+    "pdlpgpu_mps_write": (C.c_int32, [C.c_char_p, C.POINTER(Lp), C.c_char_p]),
 }
 
 _LIB = None

@@ -88,6 +88,11 @@ class Pipeline:
         L.pl_model_import.argtypes = [C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_int64,
                                       _i32p, _dp, _i32p, _dp, _dp, _dp, _dp, _i64p, _i32p, _dp]
         L.pl_model_import.restype = C.c_void_p
+        L.pl_name.argtypes = [C.c_void_p, C.c_int32, C.c_int64]
+        L.pl_name.restype = C.c_char_p
+        L.pl_warning_count.argtypes = [C.c_void_p]
+        L.pl_warning_count.restype = C.c_int64
+        L.pl_model_quadratic.argtypes = [C.c_void_p, _i32p, _i32p, _dp]
 
     # -- models --------------------------------------------------------------
     def read_mps(self, path: str) -> "Model":
@@ -124,12 +129,31 @@ class Model:
         except Exception:
             pass
 
-    def export(self) -> dict:
-        """The Model IR as flat arrays (MODEL_FIELDS)."""
+    def names(self) -> dict:
+        """Model name, variable and row names, and the reader's warnings."""
+        L = self.pl.lib
+        get = lambda kind, i: L.pl_name(self.h, kind, i).decode()   # noqa: E731
+        return dict(name=get(0, 0), variables=[get(1, j) for j in range(self.variables)],
+                    rows=[get(2, i) for i in range(self.constraints)],
+                    warnings=[get(3, k) for k in range(L.pl_warning_count(self.h))])
+
+    def quadratic(self):
+        """(i, j, value) arrays of the quadratic objective terms."""
         L = self.pl.lib
         no, nr, nq = C.c_int64(), C.c_int64(), C.c_int64()
         L.pl_model_sizes(self.h, C.byref(no), C.byref(nr), C.byref(nq))
+        i, j, v = np.zeros(nq.value, np.int32), np.zeros(nq.value, np.int32), np.zeros(nq.value)
         if nq.value:
+            L.pl_model_quadratic(self.h, _p(i, _i32p), _p(j, _i32p), _p(v, _dp))
+        return i, j, v
+
+    def export(self, allow_quadratic: bool = False) -> dict:
+        """The Model IR as flat arrays (MODEL_FIELDS); quadratic terms are not
+        carried (refused unless `allow_quadratic`)."""
+        L = self.pl.lib
+        no, nr, nq = C.c_int64(), C.c_int64(), C.c_int64()
+        L.pl_model_sizes(self.h, C.byref(no), C.byref(nr), C.byref(nq))
+        if nq.value and not allow_quadratic:
             raise ValueError("quadratic objective terms are not carried")
         sense, offset = np.zeros(1, np.int32), np.zeros(1)
         out = dict(objective_index=np.zeros(no.value, np.int32),

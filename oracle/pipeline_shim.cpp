@@ -36,6 +36,7 @@ void put(char* dst, int len, const std::string& s) {
 
 struct pl_model {
     model::Model model;
+    std::vector<std::string> warnings;   // the reader's, when read from a file
     pdlp::CompiledLp compiled;
     adapter::PdlpTranslation translation;
 };
@@ -60,7 +61,13 @@ PL_API int pl_read_mps(const char* path, pl_model** out, char* message, int mess
     try {
         mps::MpsReader reader;
         auto* h = new pl_model;
-        h->model = reader.read(path);
+        try {
+            h->model = reader.read(path);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        h->warnings = reader.warnings();
         *out = h;
         return 0;
     } catch (const std::exception& e) {
@@ -222,4 +229,29 @@ PL_API pl_model* pl_model_import(int64_t variables, int64_t constraints, int32_t
             c.linearTerms.push_back({row_index[k], row_value[k]});
     }
     return h;
+}
+
+// Names and warnings: kind 0 the model name, 1 variable `index`, 2 row
+// `index`, 3 warning `index`; NULL out of range.
+PL_API const char* pl_name(const pl_model* h, int32_t kind, int64_t index) {
+    const model::Model& m = h->model;
+    if (kind == 0) return m.name.c_str();
+    if (index < 0) return nullptr;
+    const std::size_t k = static_cast<std::size_t>(index);
+    if (kind == 1) return k < m.variables.size() ? m.variables[k].name.c_str() : nullptr;
+    if (kind == 2) return k < m.constraints.size() ? m.constraints[k].name.c_str() : nullptr;
+    if (kind == 3) return k < h->warnings.size() ? h->warnings[k].c_str() : nullptr;
+    return nullptr;
+}
+
+PL_API int64_t pl_warning_count(const pl_model* h) { return static_cast<int64_t>(h->warnings.size()); }
+
+// Quadratic objective terms in stored order.
+PL_API void pl_model_quadratic(const pl_model* h, int32_t* i, int32_t* j, double* value) {
+    const auto& q = h->model.objective.quadraticTerms;
+    for (std::size_t k = 0; k < q.size(); ++k) {
+        i[k] = q[k].variableIndex1;
+        j[k] = q[k].variableIndex2;
+        value[k] = q[k].value;
+    }
 }
