@@ -262,3 +262,95 @@ def test_reader_is_faster_than_the_reference(tmp_path, ref):
     print(f"MPS read, {lp.nnz} nonzeros, {os.path.getsize(path) / 1e6:.1f} MB: "
           f"this reader {t1 - t0:.3f} s, reference {t2 - t1:.3f} s ({(t2 - t1) / (t1 - t0):.1f}x)")
     assert t1 - t0 < t2 - t1
+
+
+FACADE_PROGRAM = r"""
+#include "mps/mps_reader.h"
+#include "pdlpgpu_mps.hpp"
+
+#include <algorithm>
+#include <cstdio>
+#include <string>
+#include <tuple>
+#include <vector>
+
+using Terms = std::vector<std::pair<int, double>>;
+
+static Terms sorted(const std::vector<model::LinearTerm>& t) {
+    Terms out;
+    for (const auto& x : t) out.emplace_back(x.variableIndex, x.value);
+    std::sort(out.begin(), out.end());
+    return out;
+}
+
+static bool same(const model::Model& a, const model::Model& b) {
+    if (a.name != b.name || a.objective.sense != b.objective.sense ||
+        a.objective.offset != b.objective.offset || a.variables.size() != b.variables.size() ||
+        a.constraints.size() != b.constraints.size() ||
+        sorted(a.objective.linearTerms) != sorted(b.objective.linearTerms) ||
+        a.objective.quadraticTerms.size() != b.objective.quadraticTerms.size())
+        return false;
+    for (size_t k = 0; k < a.objective.quadraticTerms.size(); ++k) {
+        const auto& p = a.objective.quadraticTerms[k];
+        const auto& q = b.objective.quadraticTerms[k];
+        if (p.variableIndex1 != q.variableIndex1 || p.variableIndex2 != q.variableIndex2 || p.value != q.value)
+            return false;
+    }
+    for (size_t j = 0; j < a.variables.size(); ++j) {
+        const auto& p = a.variables[j];
+        const auto& q = b.variables[j];
+        if (p.name != q.name || p.type != q.type || p.lowerBound != q.lowerBound || p.upperBound != q.upperBound)
+            return false;
+    }
+    for (size_t i = 0; i < a.constraints.size(); ++i) {
+        const auto& p = a.constraints[i];
+        const auto& q = b.constraints[i];
+        if (p.name != q.name || p.lowerBound != q.lowerBound || p.upperBound != q.upperBound ||
+            sorted(p.linearTerms) != sorted(q.linearTerms))
+            return false;
+    }
+    return true;
+}
+
+int main(int argc, char** argv) {
+    for (int f = 1; f < argc; ++f) {
+        mps::MpsReader ref;
+        pdlpgpu::MpsReader ours;
+        model::Model a, b;
+        std::string ea, eb;
+        try { a = ref.read(argv[f]); } catch (const std::exception& e) { ea = e.what(); }
+        try { b = ours.read(argv[f]); } catch (const std::exception& e) { eb = e.what(); }
+        const bool ok = ea == eb && (!ea.empty() || (same(a, b) && ref.warnings() == ours.warnings()));
+        std::printf("%s %s\n", ok ? "SAME" : "DIFFERENT", argv[f]);
+    }
+    return 0;
+}
+"""
+
+
+def test_cpp_facade_reads_like_the_reference(tmp_path):
+    """include/pdlpgpu_mps.hpp against mps::MpsReader in one C++ program built
+    from the reference's headers and reader sources: the same model::Model,
+    warnings and errors for every MPS file the reference ships."""
+    import shutil
+    import subprocess
+    root = _reference_root()
+    files = reference_files()
+    if not files or shutil.which("g++") is None:
+        pytest.skip("the reference's sources or g++ are not available here")
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib_dir = os.path.join(repo, "optimisation_solver_b200", "_lib")
+    src = tmp_path / "mps_facade.cpp"
+    src.write_text(FACADE_PROGRAM)
+    exe = tmp_path / "mps_facade"
+    cmd = ["g++", "-std=c++17", "-O1", "-I", os.path.join(repo, "include"),
+           "-I", os.path.join(root, "include"), str(src),
+           os.path.join(root, "src", "mps", "mps_reader.cpp"), os.path.join(root, "src", "model", "model.cpp"),
+           "-o", str(exe), "-L", lib_dir, "-lpdlpgpu", f"-Wl,-rpath,{lib_dir}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe), *files], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.strip().splitlines()
+    assert len(lines) == len(files)
+    assert all(line.startswith("SAME ") for line in lines), [l for l in lines if not l.startswith("SAME")]
