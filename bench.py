@@ -551,9 +551,40 @@ def extras(args, session, graph, sup, cost, inputs, value, iters, solve, family,
                                "optimal_fraction": cold["optimal"] / sup.shape[0]}
         out["learned_gain"] = {"lps_ratio": round(value / out["cold_batched"]["lps_per_s"], 3),
                                "iteration_ratio": round(float(iters.mean()) / float(cold["iterations"].mean()), 3)}
+    out["gemm"] = gemm_throughput()
     out["plain_gpu_fp64_single"] = plain_gpu(graph, inputs, args.tol)
     out["speedup_vs_plain_gpu_fp64"] = round(value / out["plain_gpu_fp64_single"]["lps_per_s"], 2)
     out["large_lp_trial_kernels"] = large_lp_kernels()
+    return out
+
+
+def gemm_throughput():
+    """The network's tensor-core GEMM alone (CUDA events, 20 calls after a
+    warm-up): an 8192^3 product and the first layer's forward shape of the
+    flow model (256 instances x 512 hidden x 22,000 features, split-K 18),
+    in TFLOP/s and as a fraction of the measured dense BF16 peak."""
+    import ctypes as C
+
+    import torch
+    from optimisation_solver_b200 import native
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = json.load(open(path)).get("bf16_tflops", 1590.0) if os.path.exists(path) else 1590.0
+    out = {"peak_tflops": peak}
+    g = torch.Generator(device="cuda").manual_seed(0)
+    for name, (M, N, K, splits) in {"square_8192": (8192, 8192, 8192, 1),
+                                    "flow_layer1_forward": (256, 512, 22000, 18)}.items():
+        a = torch.randn((M, K), device="cuda", generator=g).to(torch.bfloat16)
+        b = torch.randn((N, K), device="cuda", generator=g).to(torch.bfloat16)
+        c = torch.empty((M, N), device="cuda", dtype=torch.float32)
+        ms = C.c_double()
+        rc = native.lib().pdlpgpu_gemm_time(M, N, K, C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
+                                            C.c_void_p(c.data_ptr()), splits, 20, C.byref(ms))
+        if rc != 0:
+            out[name] = {"error": native.last_error()}
+            continue
+        tf = 2.0 * M * N * K / (ms.value * 1e-3) / 1e12
+        out[name] = {"us": round(ms.value * 1e3, 2), "tflops": round(tf, 1), "frac": round(tf / peak, 4)}
+        del a, b, c
     return out
 
 

@@ -67,6 +67,13 @@ int32_t pdlpgpu_mlp_set_params(pdlpgpu_mlp* mlp, const float* W1, const float* b
 int32_t pdlpgpu_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint16_t* A, const uint16_t* B,
                           float* C, int32_t splits);
 
+/* Measurement of the same GEMM (and, with splits > 1, the fixed-order sum of
+ * the split-K partials): one warm-up call, then `reps` calls between CUDA
+ * events on the legacy default stream; *ms_per_call is their mean. Scratch is
+ * allocated before the first event. Returns 0 or -1. */
+int32_t pdlpgpu_gemm_time(int32_t M, int32_t N, int32_t K, const uint16_t* A, const uint16_t* B,
+                          float* C, int32_t splits, int32_t reps, double* ms_per_call);
+
 /* Codec between an LP family's instances and the network (device pointers,
  * default stream). Features: the instance parameters [batch][count] (FP64)
  * standardised per feature and rounded to BF16, zero-padded to `padded`

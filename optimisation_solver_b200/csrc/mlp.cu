@@ -194,23 +194,31 @@ gemm_tn(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUten
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    bool ok = true;
-    if (threadIdx.x == 0 && nk > 0) {
+    // Warp-specialised pipeline. Lane 0 of warp 0 produces: it refills a
+    // stage as soon as the MMAs that read it have completed (`empty`), never
+    // waiting on the MMAs of other stages. Lane 0 of warp 1 consumes: it
+    // waits for a stage's bytes (`full`), issues its four MMAs and commits
+    // the stage back, so the tensor pipe always has the next stage queued.
+    __shared__ int consumed_by_mma;
+    if (threadIdx.x == 0) consumed_by_mma = 0;
+    __syncthreads();
+    int issued = 0;
+    if (warp == 0 && lane == 0 && nk > 0) {
         const uint32_t tx = STAGE_A_BYTES + STAGE_B_BYTES;
-        int issued = 0;   // stages whose TMA was issued
-        for (; issued < nk && issued < STAGES; ++issued) {
-            const int s = issued;
+        for (int i = 0; i < nk; ++i) {
+            const int s = i % STAGES;
+            if (i >= STAGES && !mbar_wait(smem_u32(&empty[s]), ((i / STAGES) - 1) & 1, a.err, 2)) break;
             const uint32_t fb = smem_u32(&full[s]);
             mbar_expect_tx(fb, tx);
-            tma_load_2d(smem_u32(sa + s * STAGE_A_BYTES), &map_a, fb, (kb0 + issued) * BK, m0);
-            tma_load_2d(smem_u32(sb + s * STAGE_B_BYTES), &map_b, fb, (kb0 + issued) * BK, n0);
+            tma_load_2d(smem_u32(sa + s * STAGE_A_BYTES), &map_a, fb, (kb0 + i) * BK, m0);
+            tma_load_2d(smem_u32(sb + s * STAGE_B_BYTES), &map_b, fb, (kb0 + i) * BK, n0);
+            ++issued;
         }
-        int consumed = 0;
-        for (int i = 0; i < nk && ok; ++i) {
+    } else if (warp == 1 && lane == 0 && nk > 0) {
+        int i = 0;
+        for (; i < nk; ++i) {
             const int s = i % STAGES;
-            const uint32_t ph = (i / STAGES) & 1;
-            if (!mbar_wait(smem_u32(&full[s]), ph, a.err, 1)) { ok = false; break; }
-            consumed = i + 1;
+            if (!mbar_wait(smem_u32(&full[s]), (i / STAGES) & 1, a.err, 1)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t a_base = smem_u32(sa + s * STAGE_A_BYTES);
             const uint32_t b_base = smem_u32(sb + s * STAGE_B_BYTES);
@@ -221,39 +229,41 @@ gemm_tn(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUten
                          (i > 0 || kk > 0) ? 1u : 0u);
             }
             mma_commit(smem_u32(&empty[s]));
-            if (i + STAGES < nk) {
-                if (!mbar_wait(smem_u32(&empty[s]), ph, a.err, 2)) { ok = false; break; }
-                const uint32_t fb = smem_u32(&full[s]);
-                mbar_expect_tx(fb, tx);
-                tma_load_2d(smem_u32(sa + s * STAGE_A_BYTES), &map_a, fb, (kb0 + i + STAGES) * BK, m0);
-                tma_load_2d(smem_u32(sb + s * STAGE_B_BYTES), &map_b, fb, (kb0 + i + STAGES) * BK, n0);
-                ++issued;
-            }
         }
-        // Drain: copies issued but not consumed (only after an error).
-        for (int i = consumed; i < issued; ++i) {
-            mbar_wait(smem_u32(&full[i % STAGES]), (i / STAGES) & 1, a.err, 3);
-        }
+        consumed_by_mma = i;
+        // Arrives once every MMA issued above has completed.
         mma_commit(smem_u32(done));
     }
     __syncthreads();
+    // After an error, copies the MMA warp never consumed may still be in
+    // flight: the producer waits for them (bounded) before the stage memory
+    // is reused below.
+    if (warp == 0 && lane == 0)
+        for (int i = consumed_by_mma; i < issued; ++i)
+            mbar_wait(smem_u32(&full[i % STAGES]), (i / STAGES) & 1, a.err, 3);
     bool have = nk > 0;
     if (have) have = mbar_wait(smem_u32(done), 0, a.err, 4);
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-    // Epilogue: warp w owns TMEM lanes [32w, 32w + 32) = output rows.
-    const int row = m0 + warp * 32 + lane;
-    float* crow = a.C + blockIdx.z * a.split_stride + static_cast<int64_t>(row) * a.N;
+    // Epilogue: warp w owns TMEM lanes [32w, 32w + 32) = output rows. Each
+    // 32 x 32 block goes through shared memory (the drained stage buffers),
+    // so every store instruction writes 32 consecutive floats of one row.
+    float* tile = reinterpret_cast<float*>(sa) + warp * 32 * 33;
+    const int row0 = m0 + warp * 32;
+    float* cbase = a.C + blockIdx.z * a.split_stride;
     for (int c0 = 0; c0 < BN; c0 += 32) {
         uint32_t r[32];
         tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + c0, r);
-        if (row < a.M) {
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const int col = n0 + c0 + j;
-                if (col < a.N) crow[col] = have ? __uint_as_float(r[j]) : 0.0f;
-            }
+        for (int j = 0; j < 32; ++j) tile[lane * 33 + j] = have ? __uint_as_float(r[j]) : 0.0f;
+        __syncwarp();
+        const int col = n0 + c0 + lane;
+        for (int rr = 0; rr < 32; ++rr) {
+            const int row = row0 + rr;
+            if (row < a.M && col < a.N) cbase[static_cast<int64_t>(row) * a.N + col] = tile[rr * 33 + lane];
         }
+        __syncwarp();
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -864,6 +874,56 @@ int32_t pdlpgpu_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint16_t* A, co
     return ok ? 0 : fail("gemm: " + (msg.empty() ? std::string(cudaGetErrorString(cudaGetLastError())) : msg));
 }
 
+
+int32_t pdlpgpu_gemm_time(int32_t M, int32_t N, int32_t K, const uint16_t* A, const uint16_t* B,
+                          float* C, int32_t splits, int32_t reps, double* ms_per_call) {
+    if (M <= 0 || N <= 0 || K <= 0 || reps <= 0 || ms_per_call == nullptr)
+        return fail("gemm_time: sizes and repetitions must be positive");
+    const int total_kb = (K + BK - 1) / BK;
+    splits = std::max(1, std::min(splits, total_kb));
+    const int per = (total_kb + splits - 1) / splits;
+    const int s_eff = (total_kb + per - 1) / per;
+    int* err = nullptr;
+    float* partial = nullptr;
+    if (cudaMalloc(&err, sizeof(int)) != cudaSuccess) return fail("gemm_time: cudaMalloc failed");
+    cudaMemset(err, 0, sizeof(int));
+    if (s_eff > 1 && cudaMalloc(&partial, sizeof(float) * static_cast<size_t>(s_eff) * M * N) != cudaSuccess) {
+        cudaFree(err);
+        return fail("gemm_time: cudaMalloc failed");
+    }
+    float* target = s_eff > 1 ? partial : C;
+    std::string msg;
+    auto once = [&]() {
+        bool ok = gemm(reinterpret_cast<const bf16*>(A), reinterpret_cast<const bf16*>(B), target, M, N, K,
+                       s_eff, err, nullptr, msg);
+        if (ok && s_eff > 1)
+            epilogue<<<grid_for(static_cast<int64_t>(M) * N), 256>>>(partial, s_eff, static_cast<int64_t>(M) * N,
+                                                                      M, N, nullptr, 0, C, nullptr);
+        return ok;
+    };
+    bool ok = once();   // warm-up: tensor maps, instruction cache
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    for (int r = 0; ok && r < reps; ++r) ok = once();
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int h = 0;
+    if (cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) ok = false;
+    if (h != 0) {
+        ok = false;
+        msg = "tensor-core pipeline wait timed out (code " + std::to_string(h) + ")";
+    }
+    cudaFree(err);
+    if (partial) cudaFree(partial);
+    *ms_per_call = ms / reps;
+    return ok ? 0 : fail("gemm_time: " + (msg.empty() ? std::string(cudaGetErrorString(cudaGetLastError())) : msg));
+}
 
 int32_t pdlpgpu_encode_features(const double* params, int32_t batch, int32_t count, int32_t padded,
                                 const float* mean, const float* inv_std, uint16_t* out) {

@@ -128,6 +128,8 @@ SIGNATURES = {
     "pdlpgpu_mlp_set_params": (C.c_int32, [C.c_void_p] + [C.c_void_p] * 6),
     "pdlpgpu_gemm_bf16": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_int32]),
+    "pdlpgpu_gemm_time": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_int32, C.c_int32, _dp]),
     "pdlpgpu_mlp_launches": (C.c_int64, [C.c_void_p]),
     "pdlpgpu_encode_features": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
                                             C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -141,3 +141,35 @@ def test_training_reduces_loss():
     for _ in range(60):
         last = net.train_step(Xb, Tt, wt, 1e-3)
     assert last < 0.5 * first
+
+
+@pytest.mark.parametrize("M,N,K,splits", [(1024, 1024, 2048, 1), (256, 512, 22000, 18)])
+def test_gemm_timing_entry_point_computes_the_product(M, N, K, splits):
+    """pdlpgpu_gemm_time runs the product `reps` times between CUDA events;
+    the result left in C is the product, and the time is positive. Prints the
+    throughput against the measured dense BF16 peak."""
+    import ctypes as C
+    import json
+    import os
+
+    import torch
+    from optimisation_solver_b200 import native
+    rng = np.random.default_rng(M + N + K)
+    a = mo.bf16(rng.standard_normal((M, K)))
+    b = mo.bf16(rng.standard_normal((N, K)))
+    c = torch.empty((M, N), dtype=torch.float32, device="cuda")
+    A, B = _bf(a), _bf(b)
+    ms = C.c_double()
+    rc = native.lib().pdlpgpu_gemm_time(M, N, K, C.c_void_p(A.data_ptr()), C.c_void_p(B.data_ptr()),
+                                        C.c_void_p(c.data_ptr()), splits, 5, C.byref(ms))
+    assert rc == 0, native.last_error()
+    got = c.cpu().numpy().astype(np.float64)
+    want = a @ b.T
+    scale = (np.abs(a) @ np.abs(b).T).max()
+    assert np.abs(got - want).max() <= 1e-5 * scale
+    assert ms.value > 0.0
+    peaks = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
+    peak = json.load(open(peaks)).get("bf16_tflops", 1590.0) if os.path.exists(peaks) else 1590.0
+    tflops = 2.0 * M * N * K / (ms.value * 1e-3) / 1e12
+    print(f"gemm {M}x{N}x{K} splits {splits}: {ms.value * 1e3:.1f} us, {tflops:.1f} TFLOP/s "
+          f"({tflops / peak:.3f} of {peak})")
