@@ -37,6 +37,7 @@
 #include <stdexcept>
 #include <string>
 #include <string_view>
+#include <thread>
 #include <vector>
 
 extern "C" void pdlpgpu_internal_set_error(const char* message);
@@ -346,6 +347,7 @@ public:
             if (tok.empty()) continue;
             if (line[0] != ' ' && line[0] != '\t') {
                 if (header(tok, line_number)) break;
+                if (section_ == Section::Columns) p = columns_in_parallel(p, end, line_number);
                 continue;
             }
             record(tok, line, line_number);
@@ -442,18 +444,210 @@ private:
         if (!last_col_name_.empty() && name == last_col_name_) return last_col_;
         const int32_t before = cols_.size();
         const int32_t j = cols_.insert(name);
-        if (j == before) {
-            out_.var_names.emplace_back(name);
-            out_.var_type.push_back(integer_marker_ ? kInteger : kContinuous);
-            out_.var_lower.push_back(0.0);
-            out_.var_upper.push_back(kInf);
-            lower_explicit_.push_back(0);
-            obj_sum_.push_back(0.0);
-            obj_has_.push_back(0);
-        }
+        if (j == before) new_column(name, integer_marker_);
         last_col_name_ = name;
         last_col_ = j;
         return j;
+    }
+
+    // The variable's model entries, for a name just added to cols_.
+    void new_column(sv name, bool integer) {
+        out_.var_names.emplace_back(name);
+        out_.var_type.push_back(integer ? kInteger : kContinuous);
+        out_.var_lower.push_back(0.0);
+        out_.var_upper.push_back(kInf);
+        lower_explicit_.push_back(0);
+        obj_sum_.push_back(0.0);
+        obj_has_.push_back(0);
+    }
+
+    // ---- COLUMNS in parallel -------------------------------------------
+    // A COLUMNS section of more than kParallelBytes is cut into chunks at
+    // line boundaries, one per host thread. Its records only look rows up
+    // (the rows are final once COLUMNS starts) and create columns, so each
+    // thread resolves rows through the read-only tables and keeps its own
+    // first-appearance list of columns it has not seen created, with the
+    // integer-marker state its chunk has set so far (or "inherited"). The
+    // merge, in chunk order, creates those columns in file order with their
+    // types and appends terms, objective contributions and warnings in file
+    // order: the model, the warnings and the first error are the sequential
+    // reader's.
+    static constexpr size_t kParallelBytes = size_t(8) << 20;
+
+    struct ChunkWarn {
+        int kind;   // 0: unknown row, 1: record without coefficients
+        sv var, row;
+    };
+    struct Chunk {
+        const char* begin = nullptr;
+        const char* end = nullptr;
+        std::vector<int32_t> t_row, t_col;   // t_col >= 0: existing column; < 0: ~(local index)
+        std::vector<double> t_val;
+        std::vector<int32_t> o_col;
+        std::vector<double> o_val;
+        std::vector<sv> new_cols;
+        std::vector<int8_t> new_marker;      // -1: the state the chunk inherits
+        std::vector<ChunkWarn> warns;
+        int8_t end_marker = -1;
+        size_t lines = 0;
+        bool failed = false;
+        size_t fail_line = 0;                // within the chunk, from 1
+        std::string fail_message;
+    };
+
+    void parse_chunk(Chunk& c) const {
+        NameTable local;
+        std::vector<sv> tok;
+        int8_t marker = -1;
+        sv last_name;
+        int32_t last_ref = 0;
+        auto colref = [&](sv name) -> int32_t {
+            if (!last_name.empty() && name == last_name) return last_ref;
+            int32_t r = cols_.find(name);
+            if (r < 0) {
+                const int32_t before = local.size();
+                const int32_t k = local.insert(name);
+                if (k == before) {
+                    c.new_cols.push_back(name);
+                    c.new_marker.push_back(marker);
+                }
+                r = ~k;
+            }
+            last_name = name;
+            last_ref = r;
+            return r;
+        };
+        const char* p = c.begin;
+        while (p < c.end) {
+            const char* nl = static_cast<const char*>(std::memchr(p, '\n', static_cast<size_t>(c.end - p)));
+            const char* le = nl ? nl : c.end;
+            sv line(p, static_cast<size_t>(le - p));
+            p = nl ? nl + 1 : c.end;
+            ++c.lines;
+            if (!line.empty() && line.back() == '\r') line.remove_suffix(1);
+            if (line.empty() || line[0] == '*') continue;
+            split(line, tok);
+            if (tok.empty()) continue;
+            if (tok.size() >= 3 && keyword(tok[1], "MARKER") &&
+                (keyword(tok[2], "INTORG") || keyword(tok[2], "INTEND"))) {
+                marker = keyword(tok[2], "INTORG") ? 1 : 0;
+                c.end_marker = marker;
+                last_name = sv();
+                continue;
+            }
+            const sv var = tok[0];
+            const int32_t col = colref(var);
+            int pairs = 0;
+            for (size_t k = 1; k < tok.size(); k += 2) {
+                double value = 0.0;
+                if (k + 1 >= tok.size() || !parse_stream(tok[k + 1], value)) {
+                    c.failed = true;
+                    c.fail_line = c.lines;
+                    c.fail_message = "COLUMNS entry for '" + std::string(var) + "' row '" +
+                                     std::string(tok[k]) + "' has no coefficient";
+                    return;
+                }
+                ++pairs;
+                const sv row = tok[k];
+                if (row == objective_) {
+                    c.o_col.push_back(col);
+                    c.o_val.push_back(value);
+                    continue;
+                }
+                const int32_t i = rows_.find(row);
+                if (i >= 0) {
+                    c.t_row.push_back(i);
+                    c.t_col.push_back(col);
+                    c.t_val.push_back(value);
+                } else if (!is_free_row(row)) {
+                    c.warns.push_back({0, var, row});
+                }
+            }
+            if (pairs == 0) c.warns.push_back({1, var, sv()});
+        }
+    }
+
+    // Parses the COLUMNS section starting at `p` in parallel when it is large;
+    // returns where the sequential loop resumes (the next header, or `p`
+    // unchanged for a small section).
+    const char* columns_in_parallel(const char* p, const char* end, size_t& line_number) {
+        unsigned threads = std::thread::hardware_concurrency();
+        if (threads > 32) threads = 32;
+        if (threads < 2) return p;
+        // The section ends at the next header line.
+        const char* q = p;
+        while (q < end) {
+            const char* nl = static_cast<const char*>(std::memchr(q, '\n', static_cast<size_t>(end - q)));
+            const char* le = nl ? nl : end;
+            sv line(q, static_cast<size_t>(le - q));
+            if (!line.empty() && line.back() == '\r') line.remove_suffix(1);
+            if (!line.empty() && line[0] != '*' && line[0] != ' ' && line[0] != '\t') {
+                bool any = false;
+                for (char ch : line) any = any || !is_space(ch);
+                if (any) break;
+            }
+            q = nl ? nl + 1 : end;
+        }
+        const size_t bytes = static_cast<size_t>(q - p);
+        if (bytes < kParallelBytes) return p;
+        flush();
+        std::vector<Chunk> chunks(threads);
+        const char* b = p;
+        for (unsigned k = 0; k < threads; ++k) {
+            const char* e = k + 1 == threads ? q : p + bytes * (k + 1) / threads;
+            if (e < b) e = b;
+            if (k + 1 < threads && e < q) {
+                const char* nl = static_cast<const char*>(std::memchr(e, '\n', static_cast<size_t>(q - e)));
+                e = nl ? nl + 1 : q;
+            }
+            chunks[k].begin = b;
+            chunks[k].end = e;
+            b = e;
+        }
+        std::vector<std::thread> pool;
+        for (unsigned k = 1; k < threads; ++k) pool.emplace_back([this, &chunks, k] { parse_chunk(chunks[k]); });
+        parse_chunk(chunks[0]);
+        for (std::thread& t : pool) t.join();
+        // Merge in chunk order.
+        bool marker = integer_marker_;
+        size_t base = line_number;
+        std::vector<int32_t> map;
+        for (Chunk& c : chunks) {
+            if (c.failed) fail(c.fail_message, base + c.fail_line);
+            map.resize(c.new_cols.size());
+            for (size_t k = 0; k < c.new_cols.size(); ++k) {
+                const int32_t before = cols_.size();
+                const int32_t j = cols_.insert(c.new_cols[k]);
+                if (j == before) new_column(c.new_cols[k], c.new_marker[k] < 0 ? marker : c.new_marker[k] == 1);
+                map[k] = j;
+            }
+            if (c.end_marker >= 0) marker = c.end_marker == 1;
+            auto resolve = [&](int32_t r) { return r >= 0 ? r : map[static_cast<size_t>(~r)]; };
+            for (size_t k = 0; k < c.o_col.size(); ++k) {
+                const size_t j = static_cast<size_t>(resolve(c.o_col[k]));
+                obj_sum_[j] += c.o_val[k];
+                obj_has_[j] = 1;
+            }
+            for (int32_t& r : c.t_col) r = resolve(r);
+            Segment sg;
+            sg.row.swap(c.t_row);
+            sg.col.swap(c.t_col);
+            sg.val.swap(c.t_val);
+            segs_.push_back(std::move(sg));
+            for (const ChunkWarn& w : c.warns) {
+                if (w.kind == 0)
+                    warn("COLUMNS entry for '" + std::string(w.var) + "' names unknown row '" +
+                         std::string(w.row) + "'; ignored");
+                else
+                    warn("COLUMNS record for '" + std::string(w.var) + "' carried no coefficients");
+            }
+            base += c.lines;
+        }
+        segs_.emplace_back();   // later sequential terms follow the chunks
+        integer_marker_ = marker;
+        last_col_name_ = sv();
+        line_number = base;
+        return q;
     }
 
     // A term on a constraint row waits in a short FIFO while its row's slot
@@ -488,9 +682,10 @@ private:
         --pending_count_;
         const int32_t i = rows_.find_hashed(p.row, p.hash);
         if (i >= 0) {
-            t_row_.push_back(i);
-            t_col_.push_back(p.col);
-            t_val_.push_back(p.value);
+            Segment& sg = segs_.back();
+            sg.row.push_back(i);
+            sg.col.push_back(p.col);
+            sg.val.push_back(p.value);
             return;
         }
         if (!is_free_row(p.row))
@@ -700,50 +895,61 @@ private:
                 m.obj_index.push_back(static_cast<int32_t>(j));
                 m.obj_value.push_back(0.0 + obj_sum_[j]);
             }
-        // Constraint terms: a stable counting sort by row, then per row by
-        // column (stable), duplicates summed from 0.0 in file order.
-        const size_t nt = t_row_.size();
+        // Constraint terms: a stable counting sort by row over the segments in
+        // file order, then per row by column (stable), duplicates summed from
+        // 0.0 in file order.
+        size_t nt = 0;
+        for (const Segment& sg : segs_) nt += sg.row.size();
         std::vector<int64_t> start(rows + 1, 0);
-        for (size_t k = 0; k < nt; ++k) ++start[static_cast<size_t>(t_row_[k]) + 1];
+        for (const Segment& sg : segs_)
+            for (int32_t r : sg.row) ++start[static_cast<size_t>(r) + 1];
         for (size_t i = 0; i < rows; ++i) start[i + 1] += start[i];
         std::vector<int32_t> col(nt);
         std::vector<double> val(nt);
         {
             std::vector<int64_t> fill(start.begin(), start.end() - 1);
-            for (size_t k = 0; k < nt; ++k) {
-                const int64_t d = fill[static_cast<size_t>(t_row_[k])]++;
-                col[static_cast<size_t>(d)] = t_col_[k];
-                val[static_cast<size_t>(d)] = t_val_[k];
+            for (Segment& sg : segs_) {
+                for (size_t k = 0; k < sg.row.size(); ++k) {
+                    const int64_t d = fill[static_cast<size_t>(sg.row[k])]++;
+                    col[static_cast<size_t>(d)] = sg.col[k];
+                    val[static_cast<size_t>(d)] = sg.val[k];
+                }
+                std::vector<int32_t>().swap(sg.row);
+                std::vector<int32_t>().swap(sg.col);
+                std::vector<double>().swap(sg.val);
             }
         }
         m.row_start.assign(rows + 1, 0);
-        m.row_index.reserve(nt);
-        m.row_value.reserve(nt);
+        m.row_index.resize(nt);
+        m.row_value.resize(nt);
+        size_t w = 0;
         std::vector<size_t> order;
         for (size_t i = 0; i < rows; ++i) {
             const size_t b = static_cast<size_t>(start[i]), e = static_cast<size_t>(start[i + 1]);
             bool sorted = true;
             for (size_t k = b + 1; k < e && sorted; ++k) sorted = col[k - 1] < col[k];
             if (sorted) {
-                for (size_t k = b; k < e; ++k) {
-                    m.row_index.push_back(col[k]);
-                    m.row_value.push_back(0.0 + val[k]);
+                for (size_t k = b; k < e; ++k, ++w) {
+                    m.row_index[w] = col[k];
+                    m.row_value[w] = 0.0 + val[k];
                 }
             } else {
                 order.resize(e - b);
                 std::iota(order.begin(), order.end(), b);
                 std::stable_sort(order.begin(), order.end(),
                                  [&](size_t x, size_t y) { return col[x] < col[y]; });
-                for (size_t q = 0; q < order.size();) {
+                for (size_t q = 0; q < order.size(); ++w) {
                     const int32_t c = col[order[q]];
                     double sum = 0.0;
                     for (; q < order.size() && col[order[q]] == c; ++q) sum += val[order[q]];
-                    m.row_index.push_back(c);
-                    m.row_value.push_back(sum);
+                    m.row_index[w] = c;
+                    m.row_value[w] = sum;
                 }
             }
-            m.row_start[i + 1] = static_cast<int64_t>(m.row_index.size());
+            m.row_start[i + 1] = static_cast<int64_t>(w);
         }
+        m.row_index.resize(w);
+        m.row_value.resize(w);
         // Quadratic terms: by (i, j), summed in file order, zero sums dropped.
         std::vector<size_t> qo(q_lo_.size());
         std::iota(qo.begin(), qo.end(), size_t(0));
@@ -794,8 +1000,16 @@ private:
     std::vector<char> sense_, has_range_, lower_explicit_, obj_has_;
     std::vector<double> rhs_, range_, obj_sum_;
     double offset_ = 0.0;
-    std::vector<int32_t> t_row_, t_col_, q_lo_, q_hi_;
-    std::vector<double> t_val_, q_val_;
+    // Constraint terms in file order, as a list of segments: the sequential
+    // reader appends to the last one, a parallel COLUMNS section adds its
+    // chunks' arrays as they are.
+    struct Segment {
+        std::vector<int32_t> row, col;
+        std::vector<double> val;
+    };
+    std::vector<Segment> segs_ = std::vector<Segment>(1);
+    std::vector<int32_t> q_lo_, q_hi_;
+    std::vector<double> q_val_;
     Pending pending_[kAhead];
     int pending_head_ = 0, pending_count_ = 0;
 };

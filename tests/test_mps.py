@@ -354,3 +354,53 @@ def test_cpp_facade_reads_like_the_reference(tmp_path):
     lines = r.stdout.strip().splitlines()
     assert len(lines) == len(files)
     assert all(line.startswith("SAME ") for line in lines), [l for l in lines if not l.startswith("SAME")]
+
+
+def _big_columns_text(m=2000, n=120_000, error_at=None):
+    """An MPS text whose COLUMNS section is larger than the size from which
+    the reader parses it on several threads (8 MiB): integer markers toggled
+    every 5,000 columns, a term on an undeclared row every 1,000 columns (a
+    warning), a repeated (row, column) pair every 777 columns, a record
+    without coefficients every 4,321 columns, each column's terms on two lines
+    (so chunk boundaries fall inside columns). `error_at`: the column whose
+    second line loses its coefficient."""
+    rng = np.random.default_rng(11)
+    rows = rng.integers(0, m, size=(n, 3))
+    vals = np.round(rng.standard_normal((n, 3)), 6)
+    out = ["NAME big", "ROWS", " N obj"] + [f" L r{i}" for i in range(m)] + ["COLUMNS"]
+    marker = False
+    for j in range(n):
+        if j % 5000 == 0 and j:
+            marker = not marker
+            out.append(f"    M{j}  'MARKER'  '{'INTORG' if marker else 'INTEND'}'")
+        a, b, c = rows[j]
+        out.append(f"    x{j}  obj  {vals[j, 0]}  r{a}  {vals[j, 1]}")
+        second = f"    x{j}  r{b}  {vals[j, 2]}  r{c}  {vals[j, 0]}"
+        if j == error_at:
+            second = f"    x{j}  r{b}  {vals[j, 2]}  r{c}"
+        out.append(second)
+        if j % 1000 == 7:
+            out.append(f"    x{j}  ghost  1.5")
+        if j % 777 == 3:
+            out.append(f"    x{j}  r{a}  0.25")
+        if j % 4321 == 5:
+            out.append(f"    x{j}")
+    out += ["RHS", "    rhs  r0  1", "BOUNDS", " UP bnd x0 4", "ENDATA"]
+    return "\n".join(out) + "\n"
+
+
+def test_parallel_columns_section_reads_the_same(tmp_path, ref):
+    text = _big_columns_text()
+    assert len(text) > 9 << 20
+    path = tmp_path / "big.mps"
+    path.write_text(text)
+    ours, our_error, theirs, their_error = _read_both(ref, str(path))
+    assert our_error is None and their_error is None, (our_error, their_error)
+    assert_same_model(ours, theirs)
+    assert any("ghost" in w for w in ours.warnings)
+    assert (ours.var_type == 1).any() and (ours.var_type == 0).any()
+    # An error deep in the section: the same message and line number.
+    bad = tmp_path / "bad.mps"
+    bad.write_text(_big_columns_text(error_at=97_531))
+    ours, our_error, theirs, their_error = _read_both(ref, str(bad))
+    assert their_error is not None and our_error == their_error, (our_error, their_error)
