@@ -126,7 +126,8 @@ typedef struct pdlpgpu_ext_options {
     int32_t cta_slots;             /* SpMV tuning: matrix slots per CTA (0 = autotune) */
     int32_t layout;                /* sessions: PDLPGPU_LAYOUT_* */
     int32_t lane_instances;        /* interleaved layout: instances per lane, 1, 2 or 4 (0 = auto) */
-    int32_t reserved[5];
+    int32_t two_kernel_trials;     /* 1: never fuse a check interval's trials into one cluster launch */
+    int32_t reserved[4];
 } pdlpgpu_ext_options;
 
 /* Optional warm start (this engine's extension; the reference starts from the

@@ -850,7 +850,45 @@ int Engine::timed_position(int k, int slots) const {
     return -1;
 }
 
+// Small instances run the trials of a check interval in one cluster launch
+// per precision (k_fused) instead of two launches per trial slot: up to 16
+// instances whose CTA maps take at most four rounds of a cluster's 4-group
+// CTAs, when the device can hold such a cluster.
+void Engine::choose_fused() {
+    fused_cluster_ = 0;
+    if (il_ || spec_.ext.two_kernel_trials == 1 || count_ <= 0 || count_ > 16) return;
+    int entries = 0;
+    for (int b = 0; b < count_; ++b)
+        entries = std::max({entries, info_[static_cast<size_t>(b)].a_cta_end - info_[static_cast<size_t>(b)].a_cta_begin,
+                            info_[static_cast<size_t>(b)].at_cta_end - info_[static_cast<size_t>(b)].at_cta_begin});
+    const int groups_per_cta = kFusedCtaThreads / kThreads;
+    int cluster = 1;
+    while (cluster < 8 && cluster * groups_per_cta < entries) cluster *= 2;
+    if (entries > 4 * cluster * groups_per_cta) return;
+    const int V = tuning_.vector_width;
+    const int resident = mixed_ ? std::min(fused_max_clusters<float>(V, cluster), fused_max_clusters<double>(V, cluster))
+                                : fused_max_clusters<double>(V, cluster);
+    if (resident <= 0) return;
+    fused_cluster_ = cluster;
+}
+
 void Engine::enqueue_chunk(int slots, bool fp64_stage) {
+    if (fused_cluster_ > 0) {
+        // One launch runs every instance's trials of the interval.
+        const int V = tuning_.vector_width;
+        record_timing(0);
+        if (mixed_) launch_fused<float>(g_, w32_, dopt_, V, count_, fused_cluster_, slots, stream_);
+        else launch_fused<double>(g_, w64_, dopt_, V, count_, fused_cluster_, slots, stream_);
+        launches_ += 1;
+        if (mixed_ && fp64_stage) {
+            launch_fused<double>(g_, w64_, dopt_, V, count_, fused_cluster_, slots, stream_);
+            launches_ += 1;
+        }
+        record_timing(1);
+        enqueue_check_stage(true);
+        record_timing(2);
+        return;
+    }
     // A mixed solve iterates in FP32; while some instance is in its FP64
     // stage, each slot also launches the per-instance FP64 trial kernels
     // (each kernel runs only the instances of its precision). Four slots'
@@ -958,7 +996,8 @@ bool Engine::build_graph(int slots, bool fp64_stage) {
 bool Engine::launch_chunk(int slots) {
     // h_active_[1]: instances in the FP64 stage at the last poll.
     const bool fp64 = mixed_ && h_active_[1] > 0;
-    const int per_chunk = 2 * slots * (fp64 ? 2 : 1) + check_stage_launches(true);
+    const int trial_launches = fused_cluster_ > 0 ? (fp64 ? 2 : 1) : 2 * slots * (fp64 ? 2 : 1);
+    const int per_chunk = trial_launches + check_stage_launches(true);
     if (spec_.ext.disable_graphs) {
         enqueue_chunk(slots, fp64);
         return check(cudaGetLastError(), "chunk launch");
@@ -976,6 +1015,7 @@ bool Engine::run() {
         return false;
     if (!check(cudaStreamSynchronize(stream_), "setup")) return false;
     mark("device setup");
+    choose_fused();
     const int slack = spec_.ext.chunk_slack > 0 ? spec_.ext.chunk_slack : 4;
     const int slots = chunk_slots();
     const int64_t trials_bound =

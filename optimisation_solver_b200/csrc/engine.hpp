@@ -192,6 +192,11 @@ private:
     pdlpgpu_lp family_{};
     // batch-interleaved layout of the trial kernels (sessions)
     bool il_ = false;
+    // Fused trials (k_fused): CTAs per cluster, 0 when the chunks launch two
+    // kernels per trial slot. Chosen by choose_fused() for one-LP solves and
+    // small batches.
+    int fused_cluster_ = 0;
+    void choose_fused();
     Interleaved<float> il32_{};
     Interleaved<double> il64_{};
     int32_t il_family_ = (1 << kIlVecs) - 1;   // vectors every instance takes from the family

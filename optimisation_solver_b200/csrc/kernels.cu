@@ -187,6 +187,7 @@ __device__ __forceinline__ double warp_range_sum(const double* part, int begin, 
 // every lane issues its loads of all three before the first add, so the
 // three reductions cost one round trip instead of three. Each result equals
 // warp_range_sum's for the same range (same per-lane order, same butterfly).
+template <bool kL2Only = false>
 __device__ __forceinline__ void warp_range_sums3(const double* p0, int b0, int e0, int s0, int q0,
                                                  const double* p1, int b1, int e1, int s1, int q1,
                                                  const double* p2, int b2, int e2, int s2, int q2,
@@ -200,9 +201,10 @@ __device__ __forceinline__ void warp_range_sums3(const double* p0, int b0, int e
 #pragma unroll
         for (int u = 0; u < kAhead; ++u) {
             const int o = k + 32 * u + lane;
-            v[0][u] = b0 + o < e0 ? p0[static_cast<int64_t>(b0 + o) * s0 + q0] : 0.0;
-            v[1][u] = b1 + o < e1 ? p1[static_cast<int64_t>(b1 + o) * s1 + q1] : 0.0;
-            v[2][u] = b2 + o < e2 ? p2[static_cast<int64_t>(b2 + o) * s2 + q2] : 0.0;
+            auto get = [](const double* p) { return kL2Only ? __ldcg(p) : *p; };
+            v[0][u] = b0 + o < e0 ? get(p0 + static_cast<int64_t>(b0 + o) * s0 + q0) : 0.0;
+            v[1][u] = b1 + o < e1 ? get(p1 + static_cast<int64_t>(b1 + o) * s1 + q1) : 0.0;
+            v[2][u] = b2 + o < e2 ? get(p2 + static_cast<int64_t>(b2 + o) * s2 + q2) : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < kAhead; ++u) {
@@ -399,6 +401,235 @@ __global__ void __launch_bounds__(kThreads, 4) k_dual(Global g, Work<T> w, Devic
                          g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 0,
                          g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 1, sums);
         if (threadIdx.x == 0) trial_control(c, so, sums[0], sums[1], sums[2], inf.n);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused trials of small LPs: one thread-block cluster per instance runs the
+// trials of a check interval in one launch. CTA rank r of the cluster serves
+// the instance's CTA-map entries r * kFusedGroups + q, stepping by the
+// cluster's group count, with its group q of 256 threads; per trial:
+//   primal half of every entry (k_primal's arithmetic, its partial per entry)
+//   cluster barrier
+//   dual half of every entry (k_dual's arithmetic)
+//   cluster barrier
+//   rank 0: the three sums in k_dual's fixed order and trial_control
+//   cluster barrier
+// so an instance's results are the two-kernel path's bit for bit, without a
+// launch, an arrival counter or a trip through the decision's dependent loads
+// per half. Vectors another CTA writes inside the launch (the iterates, the
+// partials, the control block) are read through L2 (ld.cg); the barrier's
+// release and acquire order them. Every CTA of a cluster reads the same
+// control block after the same barrier, so all of them leave the loop
+// together.
+// ---------------------------------------------------------------------------
+constexpr int kFusedGroups = 4;
+constexpr int kFusedThreads = kFusedGroups * kThreads;
+
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t cluster_size() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+
+// block_sum over one 256-thread group (its warps added in warp order, as
+// block_sum adds a CTA's); the result is valid in the group's thread 0.
+// Named barrier 1 + group; a second barrier frees `red` for the next call.
+template <int NQ>
+__device__ __forceinline__ void group_sum(double (&v)[NQ], double (*red)[kWarps], int group, int lt) {
+    const int lane = lt & 31, warp = lt >> 5;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(kFull, v[q], o);
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) red[q][warp] = v[q];
+    }
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + group), "r"(kThreads) : "memory");
+    if (lt == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double t = 0.0;
+            for (int w = 0; w < kWarps; ++w) t += red[q][w];
+            v[q] = t;
+        }
+    }
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + group), "r"(kThreads) : "memory");
+}
+
+struct FusedCtl {
+    int active, parity, pending;
+    double mult_primal, mult_dual, frac;
+};
+
+template <class T, int V>
+__device__ __forceinline__ double fused_primal(const Global& g, const Work<T>& w, const CtaWork& cw,
+                                               const InstanceInfo& inf, const FusedCtl& f, int lt) {
+    const int p = f.parity;
+    const T mult = static_cast<T>(f.mult_primal);
+    const bool pending = f.pending != 0;
+    const T frac = static_cast<T>(f.frac);
+    const T* y = w.Y[p] + inf.row_off;
+    const T* x = w.X[p] + inf.col_off;
+    T* xt = w.X[p ^ 1] + inf.col_off;
+    const T* cv = w.c + inf.col_off;
+    const T* lo = w.xl + inf.col_off;
+    const T* hi = w.xu + inf.col_off;
+    const T* tau = w.tau + inf.col_off;
+    const T* itau = w.itau + inf.col_off;
+    T* avg = w.avg_x + inf.col_off;
+    const T* vals = matrix_values<T>(g.at);
+    double moved = 0.0;
+    const int warp = lt >> 5, lane = lt & 31;
+    for (int s = cw.slice_begin + warp; s < cw.slice_end; s += kWarps) {
+        const SliceDesc sd = g.at.slices[s];
+        const LanePos lp = lane_pos(sd, lane);
+        const bool owner = lp.valid && lp.g == 0;
+        const int j = lp.line;
+        const int len = lp.valid ? g.at.line_len[inf.at_len_base + j] : 0;
+        T cj = T(0), prev = T(0), loj = T(0), hij = T(0), tj = T(0), itj = T(0), aj = T(0);
+        if (owner) {
+            cj = cv[j];
+            prev = __ldcg(x + j);
+            loj = lo[j];
+            hij = hi[j];
+            tj = tau[j];
+            itj = itau[j];
+            if (pending) aj = __ldcg(avg + j);
+        }
+        T sum[1] = {T(0)};
+        line_sums<V, 1>(inf.at_data_base + static_cast<int64_t>(sd.data_off) * 32, sd.steps, lp, lane, len,
+                        g.at.idx, vals, sum, [&](T (&a)[1], T v, int i) { a[0] += v * __ldcg(y + i); });
+        if (owner) {
+            const T gradient = cj + sum[0];
+            const T upd = smax(loj, smin(prev - mult * tj * gradient, hij));
+            xt[j] = upd;
+            const double d = static_cast<double>(upd - prev);
+            moved += d * d * static_cast<double>(itj);
+            if (pending) avg[j] = aj + frac * (prev - aj);
+        }
+    }
+    return moved;
+}
+
+template <class T, int V>
+__device__ __forceinline__ void fused_dual(const Global& g, const Work<T>& w, const CtaWork& cw,
+                                           const InstanceInfo& inf, const FusedCtl& f, int lt,
+                                           double (&red)[2]) {
+    const int p = f.parity;
+    const T dm = static_cast<T>(f.mult_dual);
+    const bool pending = f.pending != 0;
+    const T frac = static_cast<T>(f.frac);
+    const T* xt = w.X[p ^ 1] + inf.col_off;
+    const T* y = w.Y[p] + inf.row_off;
+    T* yt = w.Y[p ^ 1] + inf.row_off;
+    const T* ax = w.AX[p] + inf.row_off;
+    T* axt = w.AX[p ^ 1] + inf.row_off;
+    const T* lo = w.rl + inf.row_off;
+    const T* hi = w.ru + inf.row_off;
+    const T* sig = w.sigma + inf.row_off;
+    const T* isig = w.isigma + inf.row_off;
+    T* avg = w.avg_y + inf.row_off;
+    const T* vals = matrix_values<T>(g.a);
+    const int warp = lt >> 5, lane = lt & 31;
+    for (int s = cw.slice_begin + warp; s < cw.slice_end; s += kWarps) {
+        const SliceDesc sd = g.a.slices[s];
+        const LanePos lp = lane_pos(sd, lane);
+        const bool owner = lp.valid && lp.g == 0;
+        const int i = lp.line;
+        const int len = lp.valid ? g.a.line_len[inf.a_len_base + i] : 0;
+        T axi = T(0), sgi = T(0), prev = T(0), loi = T(0), hii = T(0), isi = T(0), ai = T(0);
+        if (owner) {
+            axi = __ldcg(ax + i);
+            sgi = sig[i];
+            prev = __ldcg(y + i);
+            loi = lo[i];
+            hii = hi[i];
+            isi = isig[i];
+            if (pending) ai = __ldcg(avg + i);
+        }
+        T sum[1] = {T(0)};
+        line_sums<V, 1, true>(inf.a_data_base + static_cast<int64_t>(sd.data_off) * 32, sd.steps, lp, lane, len,
+                              g.a.idx, vals, sum, [&](T (&a)[1], T v, int j) { a[0] += v * __ldcg(xt + j); });
+        if (owner) {
+            const T next = sum[0];
+            const T dact = next - axi;
+            const T ext = next + dact;
+            const T step = smax(dm * sgi, min_dual_step<T>());
+            const T v = prev + step * ext;
+            const T upd = smax(v - step * hii, T(0)) + smin(v - step * loi, T(0));
+            yt[i] = upd;
+            axt[i] = next;
+            const double d = static_cast<double>(upd - prev);
+            red[0] += d * d * static_cast<double>(isi);
+            red[1] += d * static_cast<double>(dact);
+            if (pending) avg[i] = ai + frac * (prev - ai);
+        }
+    }
+}
+
+template <class T, int V>
+__global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w, DeviceOptions o,
+                                                           int max_trials) {
+    __shared__ DeviceOptions so;
+    __shared__ FusedCtl f;
+    __shared__ double red[kFusedGroups][2][kWarps];
+    const uint32_t C = cluster_size(), rank = cluster_rank();
+    const int b = static_cast<int>(blockIdx.x / C);
+    const int group = threadIdx.x / kThreads, lt = threadIdx.x % kThreads;
+    InstanceCtl* cp = g.ctl + b;
+    const InstanceInfo inf = g.info[b];
+    const int stride = static_cast<int>(C) * kFusedGroups;
+    const int slot = static_cast<int>(rank) * kFusedGroups + group;
+    if (threadIdx.x == 0) so = o;
+    for (int t = 0; t < max_trials; ++t) {
+        if (threadIdx.x == 0) {
+            const volatile InstanceCtl* vc = cp;
+            const int phase = vc->phase, stage = vc->stage, fp64 = vc->fp64_stage;
+            f.active = phase != kPhaseDone && stage == kStageTrial && (fp64 != 0) == (sizeof(T) == 8);
+            f.parity = vc->parity;
+            f.pending = vc->pending_avg;
+            const double eta = vc->trial_eta, omega = vc->trial_omega;
+            f.mult_primal = eta / omega;
+            f.mult_dual = eta * omega;
+            f.frac = vc->avg_frac;
+        }
+        __syncthreads();
+        if (!f.active) break;
+        for (int e = inf.at_cta_begin + slot; e < inf.at_cta_end; e += stride) {
+            double moved[1] = {fused_primal<T, V>(g, w, g.at.ctas[e], inf, f, lt)};
+            group_sum<1>(moved, red[group], group, lt);
+            if (lt == 0) g.part_primal[e] = moved[0];
+        }
+        cluster_sync_all();
+        for (int e = inf.a_cta_begin + slot; e < inf.a_cta_end; e += stride) {
+            double r2[2] = {0.0, 0.0};
+            fused_dual<T, V>(g, w, g.a.ctas[e], inf, f, lt, r2);
+            group_sum<2>(r2, red[group], group, lt);
+            if (lt == 0) {
+                g.part_dual[2 * e] = r2[0];
+                g.part_dual[2 * e + 1] = r2[1];
+            }
+        }
+        cluster_sync_all();
+        if (rank == 0 && threadIdx.x < 32) {
+            double sums[3];
+            warp_range_sums3<true>(g.part_primal, inf.at_cta_begin, inf.at_cta_end, 1, 0,
+                                   g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 0,
+                                   g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 1, sums);
+            if (threadIdx.x == 0) trial_control(*cp, so, sums[0], sums[1], sums[2], inf.n);
+        }
+        cluster_sync_all();
     }
 }
 
@@ -1419,6 +1650,65 @@ void launch_primal(const Global& g, const Work<T>& w, const DeviceOptions&, int 
     }
 }
 
+namespace {
+template <class T, int V>
+cudaError_t fused_v(const Global& g, const Work<T>& w, const DeviceOptions& o, int count, int cluster,
+                    int max_trials, cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(count * cluster));
+    cfg.blockDim = dim3(kFusedThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = static_cast<unsigned>(cluster);
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_fused<T, V>, g, w, o, max_trials);
+}
+
+template <class T, int V>
+int fused_clusters_v(int cluster) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(cluster));
+    cfg.blockDim = dim3(kFusedThreads);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = static_cast<unsigned>(cluster);
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_fused<T, V>, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+}  // namespace
+
+template <class T>
+cudaError_t launch_fused(const Global& g, const Work<T>& w, const DeviceOptions& o, int vw, int count,
+                         int cluster, int max_trials, cudaStream_t s) {
+    if (count <= 0) return cudaSuccess;
+    switch (vw) {
+        case 4: return fused_v<T, 4>(g, w, o, count, cluster, max_trials, s);
+        case 2: return fused_v<T, 2>(g, w, o, count, cluster, max_trials, s);
+        default: return fused_v<T, 1>(g, w, o, count, cluster, max_trials, s);
+    }
+}
+
+template <class T>
+int fused_max_clusters(int vw, int cluster) {
+    switch (vw) {
+        case 4: return fused_clusters_v<T, 4>(cluster);
+        case 2: return fused_clusters_v<T, 2>(cluster);
+        default: return fused_clusters_v<T, 1>(cluster);
+    }
+}
+
 template <class T>
 void launch_dual(const Global& g, const Work<T>& w, const DeviceOptions& o, int vw, cudaStream_t s) {
     if (g.a.num_ctas == 0) return;
@@ -1608,6 +1898,9 @@ void launch_slot_done(const Global& g, int32_t count, int32_t* done, cudaStream_
 
 #define PDLPGPU_INSTANTIATE(T)                                                                      \
     template void launch_primal<T>(const Global&, const Work<T>&, const DeviceOptions&, int, cudaStream_t); \
+    template cudaError_t launch_fused<T>(const Global&, const Work<T>&, const DeviceOptions&, int, int, int, \
+                                         int, cudaStream_t);                                         \
+    template int fused_max_clusters<T>(int, int);                                                    \
     template void launch_dual<T>(const Global&, const Work<T>&, const DeviceOptions&, int, cudaStream_t);   \
     template void launch_check_prep<T>(const Global&, const Work<T>&, const DeviceOptions&, cudaStream_t);  \
     template void launch_check_apply<T>(const Global&, const Work<T>&, const DeviceOptions&, cudaStream_t); \

@@ -97,6 +97,17 @@ void launch_primal(const Global& g, const Work<T>& w, const DeviceOptions& o, in
 template <class T>
 void launch_dual(const Global& g, const Work<T>& w, const DeviceOptions& o, int vw,
                  cudaStream_t s);
+// The trials of a check interval of `count` small instances in one launch:
+// one cluster of `cluster` CTAs (1024 threads each) per instance, at most
+// `max_trials` trials each, stopping at a check or the end (kernels.cu,
+// k_fused). Same results as launch_primal + launch_dual per trial.
+template <class T>
+cudaError_t launch_fused(const Global& g, const Work<T>& w, const DeviceOptions& o, int vw, int count,
+                         int cluster, int max_trials, cudaStream_t s);
+// Clusters of that shape resident at once (0: the launch is not possible).
+template <class T>
+int fused_max_clusters(int vw, int cluster);
+constexpr int kFusedCtaThreads = 1024;
 template <class T>
 void launch_check_prep(const Global& g, const Work<T>& w, const DeviceOptions& o, cudaStream_t s);
 void launch_check_spmv(const Global& g, const DeviceOptions& o, int vw, cudaStream_t s);

@@ -57,7 +57,8 @@ class ExtOptions(C.Structure):
                 ("vector_width", C.c_int32), ("chunk_slack", C.c_int32),
                 ("fp32_stall_checks", C.c_int32), ("fp32_switch_factor", C.c_int32),
                 ("disable_graphs", C.c_int32), ("cta_slots", C.c_int32),
-                ("layout", C.c_int32), ("lane_instances", C.c_int32), ("reserved", C.c_int32 * 5)]
+                ("layout", C.c_int32), ("lane_instances", C.c_int32),
+                ("two_kernel_trials", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class WarmStart(C.Structure):
