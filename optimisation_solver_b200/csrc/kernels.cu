@@ -426,8 +426,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_dual(Global g, Work<T> w, Devic
 constexpr int kFusedGroups = 4;
 constexpr int kFusedThreads = kFusedGroups * kThreads;
 
+// Every thread of every CTA of the cluster; the warp is reconverged first
+// (the decision runs in one thread of rank 0's first warp just before).
 __device__ __forceinline__ void cluster_sync_all() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    __syncwarp();
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
 }
 
 __device__ __forceinline__ uint32_t cluster_rank() {
