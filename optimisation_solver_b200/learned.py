@@ -171,8 +171,28 @@ def train_flow_model(graph, count: int, tol: float = 1e-4, precision: str = "mix
                      out["final_primal_weight"][ok], epochs=epochs, lr=lr, lr_final=lr_final,
                      log=log)
     t2 = time.perf_counter()
+    base = baseline_loss(graph, out["primal"][ok], out["dual"][ok], out["final_primal_weight"][ok])
     info = dict(instances=int(count), solved=int(ok.sum()), label_tolerance=tol,
                 label_precision=precision, label_seconds=round(t1 - t0, 2),
                 label_mean_iterations=float(out["iterations"].mean()),
-                train_seconds=round(t2 - t1, 2), epochs=epochs, final_loss=float(hist[-1]))
+                train_seconds=round(t2 - t1, 2), epochs=epochs, final_loss=float(hist[-1]),
+                baseline_loss=base, explained_fraction=1.0 - float(hist[-1]) / base)
     return model, info
+
+
+def baseline_loss(graph, x, y, w) -> float:
+    """The training loss of the best constant prediction (each target's mean):
+    the loss weights each flow by 1/n and each potential by 1/m and the
+    log-weight by 1, over flows as capacity fractions, potentials centred per
+    instance and standardised per node, and the standardised log-weight
+    (FlowWarmStart.fit's encoding), so this is the weighted sum of the
+    targets' variances. `explained_fraction` = 1 - final_loss / this."""
+    xf = x / graph.capacity[None, :]
+    yc = y - y.mean(axis=1, keepdims=True)
+    ys = yc.std(axis=0)
+    ys[ys < 1e-12] = 1.0
+    yz = (yc - yc.mean(axis=0)) / ys
+    lw = np.log(np.maximum(w, 1e-12))
+    lz = (lw - lw.mean()) / max(lw.std(), 1e-3)
+    n, m = xf.shape[1], yz.shape[1]
+    return float(xf.var(axis=0).sum() / n + yz.var(axis=0).sum() / m + lz.var())

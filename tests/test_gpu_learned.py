@@ -52,11 +52,13 @@ def trained():
 
 
 def test_training_fits_the_labels(trained):
+    """The final loss against the constant predictor's (the weighted sum of
+    the targets' variances): the network must explain a clear share."""
     info = trained["info"]
     assert info["solved"] == info["instances"]
-    # The loss is a weighted MSE on standardised targets: a network that
-    # learned nothing sits at about 1.
-    assert info["final_loss"] < 0.9, info
+    print(f"final loss {info['final_loss']:.4f}, constant predictor {info['baseline_loss']:.4f}, "
+          f"explained {info['explained_fraction']:.3f}")
+    assert info["explained_fraction"] > 0.3, info
 
 
 def test_warm_start_needs_fewer_iterations_than_cold(trained):
