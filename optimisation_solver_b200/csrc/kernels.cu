@@ -243,6 +243,41 @@ __device__ __forceinline__ bool arrive_last(int32_t* counter, int expected) {
 }
 
 
+// Non-binding L2 prefetch of [p, p + bytes), shrunk inward to 16-byte
+// boundaries (so it never reaches outside the range) and cut into pieces of at
+// most 32 KiB spread over the CTA's threads starting at thread `first`.
+__device__ __forceinline__ void prefetch_range(const void* p, int64_t bytes, int first) {
+    if (bytes <= 0) return;
+    const uintptr_t a = (reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15);
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + static_cast<uintptr_t>(bytes)) & ~uintptr_t(15);
+    if (e <= a) return;
+    constexpr uintptr_t kPiece = 32768;
+    const uintptr_t pieces = (e - a + kPiece - 1) / kPiece;
+    for (uintptr_t k = (threadIdx.x + blockDim.x - static_cast<unsigned>(first) % blockDim.x) % blockDim.x;
+         k < pieces; k += blockDim.x) {
+        const uintptr_t b = a + k * kPiece;
+        const uint32_t n = static_cast<uint32_t>(e - b < kPiece ? e - b : kPiece);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b), "r"(n) : "memory");
+    }
+}
+
+// The streams a SELL CTA reads once: its slices' index and value data and the
+// per-line vectors of its contiguous line range, prefetched into L2 when the
+// CTA starts, so its later slices find them there.
+template <class T, int NV>
+__device__ __forceinline__ void prefetch_cta(const Side& side, const CtaWork& cw, int64_t data_base,
+                                             const T* vals, const T* const (&vecs)[NV], int nvec) {
+    if (cw.slice_end <= cw.slice_begin) return;
+    const SliceDesc first = side.slices[cw.slice_begin], last = side.slices[cw.slice_end - 1];
+    const int64_t e0 = data_base + static_cast<int64_t>(first.data_off) * 32;
+    const int64_t e1 = data_base + (static_cast<int64_t>(last.data_off) + last.steps) * 32;
+    prefetch_range(side.idx + e0, (e1 - e0) * 4, 0);
+    prefetch_range(vals + e0, (e1 - e0) * static_cast<int64_t>(sizeof(T)), 64);
+    const int l0 = first.line0, l1 = last.line0 + slice_lines(last.meta);
+    for (int v = 0; v < nvec; ++v)
+        prefetch_range(vecs[v] + l0, static_cast<int64_t>(l1 - l0) * static_cast<int64_t>(sizeof(T)), 128 + 16 * v);
+}
+
 __device__ __forceinline__ bool check_have_avg(const InstanceCtl& c, const DeviceOptions& o) {
     if (c.check_kind == kCheckInitial) return c.have_avg_at_check != 0;
     return o.averaging && c.avg_weight != 0.0;
@@ -277,6 +312,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_primal(Global g, Work<T> w) {
     const T* __restrict__ itau = w.itau + inf.col_off;
     T* __restrict__ avg = w.avg_x + inf.col_off;
     const T* vals = matrix_values<T>(g.at);
+    {
+        const T* const vecs[7] = {x, cv, lo, hi, tau, itau, avg};
+        prefetch_cta<T, 7>(g.at, cw, inf.at_data_base, vals, vecs, pending ? 7 : 6);
+    }
 
     double moved[1] = {0.0};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -340,6 +379,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_dual(Global g, Work<T> w, Devic
     const T* __restrict__ isig = w.isigma + inf.row_off;
     T* __restrict__ avg = w.avg_y + inf.row_off;
     const T* vals = matrix_values<T>(g.a);
+    {
+        const T* const vecs[7] = {ax, y, lo, hi, sig, isig, avg};
+        prefetch_cta<T, 7>(g.a, cw, inf.a_data_base, vals, vecs, pending ? 7 : 6);
+    }
 
     double red[2] = {0.0, 0.0};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
