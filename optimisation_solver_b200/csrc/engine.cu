@@ -785,6 +785,17 @@ bool Engine::power_iteration() {
     return check(cudaGetLastError(), "power iteration");
 }
 
+// A time limit as the device clocks it: nanoseconds, 0 for none. A positive
+// limit is at least 1 ns (so 1e-30 s is a limit that has passed when the
+// first loop top is reached, as in the reference, pdlp_solver.cpp:277-285);
+// one beyond the int64 range is none.
+static int64_t deadline_ns_of(double seconds) {
+    if (!(seconds > 0.0)) return 0;
+    const double ns = seconds * 1e9;
+    if (!(ns < 9.0e18)) return 0;
+    return std::max<int64_t>(1, static_cast<int64_t>(ns));
+}
+
 bool Engine::start() {
     if (!setup_ok_) return false;
     if (count_ == 0) return true;
@@ -793,8 +804,7 @@ bool Engine::start() {
     if (!spec_.opt.use_diagonal_preconditioning && !power_iteration()) return false;
     const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
     const double limit = spec_.opt.time_limit_seconds;
-    launch_stamp_clock(g_, count_, static_cast<int64_t>(elapsed * 1e9),
-                       limit > 0.0 ? static_cast<int64_t>(limit * 1e9) : 0, stream_);
+    launch_stamp_clock(g_, count_, static_cast<int64_t>(elapsed * 1e9), deadline_ns_of(limit), stream_);
     // Initial A x (refresh is gated on need_refresh, set by init_control),
     // then the initial score (pdlp_solver.cpp:239-264).
     if (mixed_) launch_refresh<float>(g_, w32_, dopt_, tuning_.vector_width, stream_);
@@ -852,7 +862,7 @@ int Engine::timed_position(int k, int slots) const {
 
 // Small instances run the trials of a check interval in one cluster launch
 // per precision (k_fused) instead of two launches per trial slot: up to 16
-// instances whose CTA maps take at most four rounds of a cluster's 4-group
+// instances whose CTA maps take at most four rounds of a cluster's 2-group
 // CTAs, when the device can hold such a cluster.
 void Engine::choose_fused() {
     fused_cluster_ = 0;
@@ -862,13 +872,17 @@ void Engine::choose_fused() {
         entries = std::max({entries, info_[static_cast<size_t>(b)].a_cta_end - info_[static_cast<size_t>(b)].a_cta_begin,
                             info_[static_cast<size_t>(b)].at_cta_end - info_[static_cast<size_t>(b)].at_cta_begin});
     const int groups_per_cta = kFusedCtaThreads / kThreads;
-    int cluster = 1;
-    while (cluster < 8 && cluster * groups_per_cta < entries) cluster *= 2;
-    if (entries > 4 * cluster * groups_per_cta) return;
     const int V = tuning_.vector_width;
-    const int resident = mixed_ ? std::min(fused_max_clusters<float>(V, cluster), fused_max_clusters<double>(V, cluster))
-                                : fused_max_clusters<double>(V, cluster);
-    if (resident <= 0) return;
+    auto resident = [&](int cluster) {
+        return mixed_ ? std::min(fused_max_clusters<float>(V, cluster), fused_max_clusters<double>(V, cluster))
+                      : fused_max_clusters<double>(V, cluster);
+    };
+    // The smallest cluster that serves every entry in one round, up to 16
+    // CTAs (8 where the device cannot hold 16), then at most four rounds.
+    int cluster = 1;
+    while (cluster < 16 && cluster * groups_per_cta < entries) cluster *= 2;
+    if (cluster == 16 && resident(16) <= 0) cluster = 8;
+    if (entries > 4 * cluster * groups_per_cta || resident(cluster) <= 0) return;
     fused_cluster_ = cluster;
 }
 
@@ -1494,9 +1508,7 @@ bool Engine::session_solve(int32_t* optimal) {
                     family_.objective_offset, stream_);
     launch_setup_vectors<double>(g_, w64_, stream_);
     if (mixed_) launch_setup_vectors<float>(g_, w32_, stream_);
-    launch_stamp_clock(g_, count_, 0,
-                       o.time_limit_seconds > 0.0 ? static_cast<int64_t>(o.time_limit_seconds * 1e9) : 0,
-                       stream_);
+    launch_stamp_clock(g_, count_, 0, deadline_ns_of(o.time_limit_seconds), stream_);
     if (mixed_) launch_refresh<float>(g_, w32_, dopt_, tuning_.vector_width, stream_);
     launch_refresh<double>(g_, w64_, dopt_, tuning_.vector_width, stream_);
     const int64_t before = launches_;
@@ -1753,8 +1765,7 @@ bool Engine::session_stream(bool on_device, int64_t N, const double* const in[5]
         if (mixed_) launch_setup_vectors<float>(gm, w32_, stream_);
         const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
         (void)elapsed;
-        launch_stamp_clock(gm, B, 0, o.time_limit_seconds > 0.0 ? static_cast<int64_t>(o.time_limit_seconds * 1e9) : 0,
-                           stream_);
+        launch_stamp_clock(gm, B, 0, deadline_ns_of(o.time_limit_seconds), stream_);
         if (mixed_) launch_refresh<float>(g_, w32_, dopt_, tuning_.vector_width, stream_);
         launch_refresh<double>(g_, w64_, dopt_, tuning_.vector_width, stream_);
         enqueue_check_stage();

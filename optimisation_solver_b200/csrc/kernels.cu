@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_dual(Global g, Work<T> w, Devic
 // control block after the same barrier, so all of them leave the loop
 // together.
 // ---------------------------------------------------------------------------
-constexpr int kFusedGroups = 4;
+constexpr int kFusedGroups = 2;   // 512 threads: up to 128 registers each
 constexpr int kFusedThreads = kFusedGroups * kThreads;
 
 // Every thread of every CTA of the cluster; the warp is reconverged first
@@ -624,12 +624,55 @@ __device__ __forceinline__ void fused_dual(const Global& g, const Work<T>& w, co
     }
 }
 
+// Distributed shared memory: the address of `local` in rank 0's shared
+// memory, and loads and stores there.
+__device__ __forceinline__ uint32_t rank0_addr(const void* local) {
+    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(local));
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(0));
+    return r;
+}
+__device__ __forceinline__ void st_cluster(uint32_t addr, double v) {
+    asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v) : "memory");
+}
+__device__ __forceinline__ double ld_cluster_f64(uint32_t addr) {
+    double v;
+    asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(addr) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_cluster_i32(uint32_t addr) {
+    int v;
+    asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+    return v;
+}
+
+// The next trial's snapshot of an instance's control block.
+__device__ __forceinline__ void fused_snapshot(const InstanceCtl& c, FusedCtl& f, bool fp64) {
+    f.active = c.phase != kPhaseDone && c.stage == kStageTrial && (c.fp64_stage != 0) == fp64;
+    f.parity = c.parity;
+    f.pending = c.pending_avg;
+    f.mult_primal = c.trial_eta / c.trial_omega;
+    f.mult_dual = c.trial_eta * c.trial_omega;
+    f.frac = c.avg_frac;
+}
+
+constexpr int kFusedMaxEntries = 4 * 16 * kFusedGroups;   // four rounds of the largest cluster
+
 template <class T, int V>
 __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w, DeviceOptions o,
                                                            int max_trials) {
+    // Rank 0 keeps the instance's control block in its shared memory for the
+    // whole launch (the decision's reads and writes stay on chip), publishes
+    // each trial's snapshot in `f`, and receives every group's partial sums in
+    // `part_p` / `part_d` through distributed shared memory; the other CTAs
+    // read `f` from rank 0 after each barrier. The block goes back to global
+    // memory when the launch ends.
     __shared__ DeviceOptions so;
     __shared__ FusedCtl f;
     __shared__ double red[kFusedGroups][2][kWarps];
+    __shared__ alignas(16) InstanceCtl sctl;
+    __shared__ double part_p[kFusedMaxEntries];
+    __shared__ double part_d[2 * kFusedMaxEntries];
     const uint32_t C = cluster_size(), rank = cluster_rank();
     const int b = static_cast<int>(blockIdx.x / C);
     const int group = threadIdx.x / kThreads, lt = threadIdx.x % kThreads;
@@ -637,25 +680,34 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
     const InstanceInfo inf = g.info[b];
     const int stride = static_cast<int>(C) * kFusedGroups;
     const int slot = static_cast<int>(rank) * kFusedGroups + group;
+    constexpr bool kFp64 = sizeof(T) == 8;
     if (threadIdx.x == 0) so = o;
+    if (rank == 0) {
+        static_assert(sizeof(InstanceCtl) % 16 == 0, "the control block copies as 16-byte words");
+        if (threadIdx.x < sizeof(InstanceCtl) / 16)
+            reinterpret_cast<int4*>(&sctl)[threadIdx.x] = reinterpret_cast<const int4*>(cp)[threadIdx.x];
+        __syncthreads();
+        if (threadIdx.x == 0) fused_snapshot(sctl, f, kFp64);
+    }
+    const uint32_t f_addr = rank0_addr(&f);
+    const uint32_t pp_addr = rank0_addr(part_p);
+    const uint32_t pd_addr = rank0_addr(part_d);
+    cluster_sync_all();
     for (int t = 0; t < max_trials; ++t) {
-        if (threadIdx.x == 0) {
-            const volatile InstanceCtl* vc = cp;
-            const int phase = vc->phase, stage = vc->stage, fp64 = vc->fp64_stage;
-            f.active = phase != kPhaseDone && stage == kStageTrial && (fp64 != 0) == (sizeof(T) == 8);
-            f.parity = vc->parity;
-            f.pending = vc->pending_avg;
-            const double eta = vc->trial_eta, omega = vc->trial_omega;
-            f.mult_primal = eta / omega;
-            f.mult_dual = eta * omega;
-            f.frac = vc->avg_frac;
+        if (rank != 0 && threadIdx.x == 0) {
+            f.active = ld_cluster_i32(f_addr + offsetof(FusedCtl, active));
+            f.parity = ld_cluster_i32(f_addr + offsetof(FusedCtl, parity));
+            f.pending = ld_cluster_i32(f_addr + offsetof(FusedCtl, pending));
+            f.mult_primal = ld_cluster_f64(f_addr + offsetof(FusedCtl, mult_primal));
+            f.mult_dual = ld_cluster_f64(f_addr + offsetof(FusedCtl, mult_dual));
+            f.frac = ld_cluster_f64(f_addr + offsetof(FusedCtl, frac));
         }
         __syncthreads();
         if (!f.active) break;
         for (int e = inf.at_cta_begin + slot; e < inf.at_cta_end; e += stride) {
             double moved[1] = {fused_primal<T, V>(g, w, g.at.ctas[e], inf, f, lt)};
             group_sum<1>(moved, red[group], group, lt);
-            if (lt == 0) g.part_primal[e] = moved[0];
+            if (lt == 0) st_cluster(pp_addr + 8u * static_cast<uint32_t>(e - inf.at_cta_begin), moved[0]);
         }
         cluster_sync_all();
         for (int e = inf.a_cta_begin + slot; e < inf.a_cta_end; e += stride) {
@@ -663,19 +715,31 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
             fused_dual<T, V>(g, w, g.a.ctas[e], inf, f, lt, r2);
             group_sum<2>(r2, red[group], group, lt);
             if (lt == 0) {
-                g.part_dual[2 * e] = r2[0];
-                g.part_dual[2 * e + 1] = r2[1];
+                const uint32_t q = 16u * static_cast<uint32_t>(e - inf.a_cta_begin);
+                st_cluster(pd_addr + q, r2[0]);
+                st_cluster(pd_addr + q + 8u, r2[1]);
             }
         }
         cluster_sync_all();
         if (rank == 0 && threadIdx.x < 32) {
+            // k_dual's fixed-order sums over the same partials, from shared memory.
             double sums[3];
-            warp_range_sums3<true>(g.part_primal, inf.at_cta_begin, inf.at_cta_end, 1, 0,
-                                   g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 0,
-                                   g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 1, sums);
-            if (threadIdx.x == 0) trial_control(*cp, so, sums[0], sums[1], sums[2], inf.n);
+            warp_range_sums3<false>(part_p, 0, inf.at_cta_end - inf.at_cta_begin, 1, 0,
+                                    part_d, 0, inf.a_cta_end - inf.a_cta_begin, 2, 0,
+                                    part_d, 0, inf.a_cta_end - inf.a_cta_begin, 2, 1, sums);
+            if (threadIdx.x == 0) {
+                trial_control(sctl, so, sums[0], sums[1], sums[2], inf.n);
+                fused_snapshot(sctl, f, kFp64);
+            }
         }
         cluster_sync_all();
+    }
+    // Every CTA left the loop at the same trial; the barrier keeps rank 0's
+    // shared memory alive until the others have read `f` from it.
+    cluster_sync_all();
+    if (rank == 0) {
+        if (threadIdx.x < sizeof(InstanceCtl) / 16)
+            reinterpret_cast<int4*>(cp)[threadIdx.x] = reinterpret_cast<const int4*>(&sctl)[threadIdx.x];
     }
 }
 
@@ -1711,6 +1775,8 @@ cudaError_t fused_v(const Global& g, const Work<T>& w, const DeviceOptions& o, i
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    // Clusters of 16 CTAs are beyond the portable size of 8.
+    cudaFuncSetAttribute(k_fused<T, V>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     return cudaLaunchKernelEx(&cfg, k_fused<T, V>, g, w, o, max_trials);
 }
 
@@ -1726,6 +1792,11 @@ int fused_clusters_v(int cluster) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    if (cluster > 8 &&
+        cudaFuncSetAttribute(k_fused<T, V>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
     int n = 0;
     if (cudaOccupancyMaxActiveClusters(&n, k_fused<T, V>, &cfg) != cudaSuccess) {
         cudaGetLastError();

@@ -98,7 +98,7 @@ template <class T>
 void launch_dual(const Global& g, const Work<T>& w, const DeviceOptions& o, int vw,
                  cudaStream_t s);
 // The trials of a check interval of `count` small instances in one launch:
-// one cluster of `cluster` CTAs (1024 threads each) per instance, at most
+// one cluster of `cluster` CTAs (512 threads each) per instance, at most
 // `max_trials` trials each, stopping at a check or the end (kernels.cu,
 // k_fused). Same results as launch_primal + launch_dual per trial.
 template <class T>
@@ -107,7 +107,7 @@ cudaError_t launch_fused(const Global& g, const Work<T>& w, const DeviceOptions&
 // Clusters of that shape resident at once (0: the launch is not possible).
 template <class T>
 int fused_max_clusters(int vw, int cluster);
-constexpr int kFusedCtaThreads = 1024;
+constexpr int kFusedCtaThreads = 512;
 template <class T>
 void launch_check_prep(const Global& g, const Work<T>& w, const DeviceOptions& o, cudaStream_t s);
 void launch_check_spmv(const Global& g, const DeviceOptions& o, int vw, cudaStream_t s);

@@ -111,20 +111,22 @@ def test_solve_batch_uneven_planted_matches_oracle(oracle, precision, tol):
 
 SHAPES = [
     # Zipf column degrees, log-uniform magnitudes, 30% equality rows, box bounds.
-    ("large_3k", lambda: g.large_lp(0, m=3000, n=6000)),
+    ("large_3k", lambda: g.large_lp(0, m=3000, n=6000), True),
     # The same rescaled by factors in [1e-4, 1e4], 20% free variables, 10% ranged rows.
-    ("stress_3k", lambda: g.stress_lp(0, m=3000, n=6000)),
+    ("stress_3k", lambda: g.stress_lp(0, m=3000, n=6000), False),
 ]
 
 
-@pytest.mark.parametrize("name,build", SHAPES, ids=[s[0] for s in SHAPES])
+@pytest.mark.parametrize("name,build,compare_objective", SHAPES, ids=[s[0] for s in SHAPES])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_single_lp_shapes_match_reference_at_1e4(oracle, name, build, precision):
-    """Both solvers stop on the reference's relative criteria. On the stress
-    family those pass well away from the planted optimum (the reference also
-    stops 0.4% off it at this size and 18% off at 8000 rows), so the objective
-    is compared with the reference's own, within the gap bound, and the point
-    is rescored by the reference."""
+def test_single_lp_shapes_match_reference_at_1e4(oracle, name, build, compare_objective, precision):
+    """Both solvers stop on the reference's relative criteria: same status, and
+    the device's point rescored by the reference's TerminationChecker meets
+    them. On the stress family those criteria pass far from the optimum and
+    the stopping point depends on rounding: the reference itself, built with
+    FMA contraction (its Release flags) and without it, stops at objectives
+    161,422.6 and 145,237.5 on this instance. There the objective is not
+    compared; on the large-LP family it is, within the gap bound."""
     tol = 1e-4
     p = build()
     opts = PdlpOptions().with_tolerance(tol)
@@ -133,7 +135,8 @@ def test_single_lp_shapes_match_reference_at_1e4(oracle, name, build, precision)
     (ref,) = solve_many(oracle, [p.lp], tol, iteration_limit=400000)
     assert str(r.status) == ref.status == "optimal", (r.status, ref.status)
     check_point(oracle, p.lp, r.primal, r.row_dual, tol)
-    check_objective(r.primal_objective, ref, tol)
+    if compare_objective:
+        check_objective(r.primal_objective, ref, tol)
 
 
 POWER_CASES = [
