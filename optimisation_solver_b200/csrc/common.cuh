@@ -178,6 +178,12 @@ struct DeviceOptions {
     double sufficient, necessary, artificial;
     double infeasibility_tol;
     double time_limit;
+    // The linesearch's step factors by iteration index k: step_pow[2k] =
+    // (k + 2)^-0.3 and step_pow[2k + 1] = (k + 2)^-0.6, computed on the
+    // device with the same pow (step_controller.cpp:30-68 needs them at
+    // every trial); indices past step_pow_entries compute them directly.
+    const double* step_pow;
+    int64_t step_pow_entries;
 };
 
 // Partial sums per elementwise CTA of a check (slot meaning depends on side).

@@ -40,8 +40,16 @@ __device__ inline bool evaluate_step(double& eta, double omega, double eta_max,
     double limit = INFINITY;
     if (coupling > 0.0 && movement > 0.0) limit = movement / (2.0 * coupling);
     const double index = static_cast<double>(iteration) + 2.0;
-    const double shrink = 1.0 - pow(index, -0.3);
-    const double grow = 1.0 + pow(index, -0.6);
+    double p3, p6;
+    if (iteration >= 0 && iteration < o.step_pow_entries) {
+        p3 = o.step_pow[2 * iteration];
+        p6 = o.step_pow[2 * iteration + 1];
+    } else {
+        p3 = pow(index, -0.3);
+        p6 = pow(index, -0.6);
+    }
+    const double shrink = 1.0 - p3;
+    const double grow = 1.0 + p6;
     const bool accepted = eta <= limit;
     double next = smin(shrink * limit, grow * eta);
     next = clampd(next, o.min_step_scale * eta_max, 1e12);

@@ -634,6 +634,18 @@ bool Engine::prepare(const SolveSpec& spec) {
     dopt_.artificial = o.restart_artificial_fraction;
     dopt_.infeasibility_tol = o.infeasibility_tolerance;
     dopt_.time_limit = o.time_limit_seconds;
+    {
+        // Step factors for every iteration index a solve can reach (main loop
+        // and polishing), at most 2^20 of them (16 MiB).
+        const int64_t reach = std::max<int64_t>(o.iteration_limit, o.polishing_iterations) + 2;
+        const int64_t entries = std::min<int64_t>(std::max<int64_t>(reach, 1), int64_t(1) << 20);
+        void* t = nullptr;
+        if (!check(cudaMalloc(&t, static_cast<size_t>(entries) * 2 * sizeof(double)), "cudaMalloc")) return false;
+        extra_.push_back(t);
+        launch_step_pow(static_cast<double*>(t), entries, stream_);
+        dopt_.step_pow = static_cast<const double*>(t);
+        dopt_.step_pow_entries = entries;
+    }
     setup_ok_ = true;
     mark("vector upload");
     return true;

@@ -1523,6 +1523,16 @@ __global__ void __launch_bounds__(kThreads) k_spmv(Global g, int transpose, cons
 }
 
 
+// The linesearch's step factors by iteration index (DeviceOptions::step_pow).
+__global__ void k_step_pow(double* table, int64_t entries) {
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < entries;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double index = static_cast<double>(k) + 2.0;
+        table[2 * k] = pow(index, -0.3);
+        table[2 * k + 1] = pow(index, -0.6);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Power iteration on A'A (preconditioner.cpp:82-140), used only when the
 // diagonal preconditioner is off. Per-instance state lives in ctl.dbg:
@@ -1955,6 +1965,10 @@ void launch_spmv(const Global& g, int transpose, int values, const T* v, T* out,
         case 2: k_spmv<T, 2><<<side.num_ctas, kThreads, 0, s>>>(g, transpose, vals, v, out); break;
         default: k_spmv<T, 1><<<side.num_ctas, kThreads, 0, s>>>(g, transpose, vals, v, out); break;
     }
+}
+
+void launch_step_pow(double* table, int64_t entries, cudaStream_t s) {
+    if (entries > 0) k_step_pow<<<blocks_for(entries, 256), 256, 0, s>>>(table, entries);
 }
 
 void launch_power_dot(const Global& g, const double* x, const double* z, cudaStream_t s) {

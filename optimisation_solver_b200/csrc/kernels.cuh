@@ -143,6 +143,8 @@ void launch_broadcast_precond(const Work<T>& w, const InstanceInfo& first, int32
                               int64_t rows, int64_t cols, cudaStream_t s);
 
 void launch_power_dot(const Global& g, const double* x, const double* z, cudaStream_t s);
+// table[2k] = (k + 2)^-0.3, table[2k + 1] = (k + 2)^-0.6 for k < entries.
+void launch_step_pow(double* table, int64_t entries, cudaStream_t s);
 void launch_power_step(const Global& g, int32_t count, int init, int it, int budget, cudaStream_t s);
 void launch_power_scale(const Global& g, double* x, const double* z, cudaStream_t s);
 void launch_power_finish(const Global& g, int32_t count, double safety, double min_scale,
