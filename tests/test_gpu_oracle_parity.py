@@ -62,8 +62,9 @@ def test_flow_stream_interleaved_matches_oracle_at_1e4(oracle, flow, precision):
 
 
 def test_flow_session_fp64_matches_oracle_objective_at_1e8(oracle, flow):
-    """FP64 mode: objectives within 1e-6 relative of the reference's, both
-    solved to 1e-8."""
+    """FP64 mode: the reference's statuses (at 1e-8 it stops one of these
+    instances at its 200,000-iteration limit too), and objectives within 1e-6
+    relative of the reference's where both are optimal."""
     G, s, c = flow
     tol, count = 1e-8, 16
     family = g.flow_lp(G, s[0], c[0])
@@ -75,10 +76,15 @@ def test_flow_session_fp64_matches_oracle_objective_at_1e8(oracle, flow):
     S.close()
     lps = [g.flow_lp(G, s[i], c[i]) for i in range(count)]
     refs = solve_many(oracle, lps, tol)
+    optimal = 0
     for i, (lp, ref) in enumerate(zip(lps, refs)):
-        assert str(out["status"][i]) == ref.status == "optimal"
+        assert str(out["status"][i]) == ref.status, (i, out["status"][i], ref.status)
+        if ref.status != "optimal":
+            continue
+        optimal += 1
         check_point(oracle, lp, out["primal"][i], out["dual"][i], tol, _scores(out, i))
         check_objective(out["primal_objective"][i], ref, tol, objective_rel=1e-6)
+    assert optimal >= count - 2
 
 
 def _uneven_planted(count=12, lo=200, hi=3000, seed=5):
