@@ -453,6 +453,8 @@ def side_workload(args, rank: int, world: int, local_rank: int):
     dev = torch.device("cuda", local_rank)
     opts = PdlpOptions().with_tolerance(args.tol)
     line = {"workload": args.workload, "tolerance": args.tol, "data": "synthetic (seeded generators)"}
+    if args.profile:
+        return side_profile(args, opts, line)
     if args.workload in ("large", "stress"):
         p = g.large_lp(0) if args.workload == "large" else g.stress_lp(0)
         line["config"] = {"rows": p.lp.num_rows, "cols": p.lp.num_cols, "nnz": int(p.lp.nnz)}
@@ -512,6 +514,31 @@ def side_workload(args, rank: int, world: int, local_rank: int):
                  "kernels": _kernel_roofline(tk), "precision": args.precision,
                  "tuned": {"params": tuned["params"], "trial_ms": round(tuned["trial_ms"], 4),
                            "default_trial_ms": round(tuned["default_trial_ms"], 4)}})
+    return line
+
+
+def side_profile(args, opts, line):
+    """`--profile` with a side workload: the two SELL-G trial kernels only,
+    timed with every instance active (no solve), for ncu captures. large /
+    stress: the one LP in FP64 then FP32, V = 1 / 4; uneven: `--count` LPs of
+    the uneven family as one batch in `--precision`, V = 4, 32 entries per
+    lane."""
+    from optimisation_solver_b200 import generators as g
+    from optimisation_solver_b200.pdlp import PdlpSolver
+    out = {}
+    if args.workload in ("large", "stress"):
+        p = g.large_lp(0) if args.workload == "large" else g.stress_lp(0)
+        line["config"] = {"rows": p.lp.num_rows, "cols": p.lp.num_cols, "nnz": int(p.lp.nnz)}
+        for prec, width in (("fp64", 1), ("mixed", 4)):
+            tk = PdlpSolver(prec, vector_width=width).time_kernels_batch([p.lp], opts, reps=20)
+            out[prec] = _kernel_roofline(tk)
+    else:
+        sizes = g.uneven_batch_sizes(args.count)
+        lps = [_planted_instance((i, sizes[i])).lp for i in range(args.count)]
+        line["config"] = {"instances": args.count, "nnz": int(sum(q.nnz for q in lps))}
+        tk = PdlpSolver(args.precision, vector_width=4, lane_elements=32).time_kernels_batch(lps, opts, reps=10)
+        out[args.precision] = _kernel_roofline(tk)
+    line["profile"] = out
     return line
 
 

@@ -999,9 +999,26 @@ __global__ void k_il_family(Interleaved<T> il, FamSrc src, const double* __restr
 
 }  // namespace
 
+// Both trial kernels ask for the largest shared-memory carveout. Left to
+// itself the driver configures each kernel's SMs for its own needs (the dual
+// needs more shared memory than the primal), and an SM switches
+// configuration only once it is empty, so a kernel's CTAs could not take the
+// place of the previous kernel's finished CTAs on a busy SM: the
+// programmatic launch lost most of its overlap. Set on the current device at
+// setup, before any launch is captured.
+template <class T, int V>
+void same_carveout() {
+    constexpr int kMaxShared = 100;   // percent
+    cudaFuncSetAttribute(k_il_primal<T, V, false>, cudaFuncAttributePreferredSharedMemoryCarveout, kMaxShared);
+    cudaFuncSetAttribute(k_il_primal<T, V, true>, cudaFuncAttributePreferredSharedMemoryCarveout, kMaxShared);
+    cudaFuncSetAttribute(k_il_dual<T, V, false>, cudaFuncAttributePreferredSharedMemoryCarveout, kMaxShared);
+    cudaFuncSetAttribute(k_il_dual<T, V, true>, cudaFuncAttributePreferredSharedMemoryCarveout, kMaxShared);
+}
+
 template <class T, int V>
 int blocks_per_sm(bool dual) {
     int r = 0;
+    same_carveout<T, V>();
     if (dual) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_il_dual<T, V, false>, kIlThreads, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_il_primal<T, V, false>, kIlThreads, 0);
     return r > 0 ? r : 1;
