@@ -188,6 +188,16 @@ __device__ inline void average_add(InstanceCtl& c, double weight) {   // iterate
     c.pending_avg = 1;
 }
 
+// A control block copied by one warp as 16-byte words (either side may be
+// shared or global memory).
+__device__ __forceinline__ void copy_ctl_warp(InstanceCtl* dst, const InstanceCtl* src) {
+    static_assert(sizeof(InstanceCtl) % 16 == 0 && sizeof(InstanceCtl) / 16 <= 32,
+                  "one 16-byte word per lane");
+    const int lane = threadIdx.x & 31;
+    if (lane < static_cast<int>(sizeof(InstanceCtl) / 16))
+        reinterpret_cast<int4*>(dst)[lane] = reinterpret_cast<const int4*>(src)[lane];
+}
+
 // After the two halves of one trial: finiteness test, linesearch decision,
 // commit, averaging and the check boundary.
 inline __device__ __noinline__ void trial_control(InstanceCtl& c, const DeviceOptions& o, double pmove,

@@ -439,11 +439,20 @@ __global__ void __launch_bounds__(kThreads, 4) k_dual(Global g, Work<T> w, Devic
     if (threadIdx.x == 0) so = o;
     __syncthreads();
     if (threadIdx.x < 32) {
+        // The decision runs on a shared-memory copy of the control block:
+        // after a store to a global line, the thread's next load of that line
+        // would be served by L2, and the decision reads back much of what it
+        // writes.
+        __shared__ alignas(16) InstanceCtl sc;
+        copy_ctl_warp(&sc, &c);
         double sums[3];
         warp_range_sums3(g.part_primal, inf.at_cta_begin, inf.at_cta_end, 1, 0,
                          g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 0,
                          g.part_dual, inf.a_cta_begin, inf.a_cta_end, 2, 1, sums);
-        if (threadIdx.x == 0) trial_control(c, so, sums[0], sums[1], sums[2], inf.n);
+        __syncwarp();
+        if (threadIdx.x == 0) trial_control(sc, so, sums[0], sums[1], sums[2], inf.n);
+        __syncwarp();
+        copy_ctl_warp(&c, &sc);
     }
 }
 

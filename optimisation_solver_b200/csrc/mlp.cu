@@ -3,12 +3,14 @@
 //
 //   gemm_tn      C[M][N] = A[M][K] * B[N][K]^T, BF16 operands, FP32
 //                accumulation on the 5th-generation tensor cores: TMA
-//                (cp.async.bulk.tensor, 128-byte swizzle) fills a 4-stage
+//                (cp.async.bulk.tensor, 128-byte swizzle) fills a 3-stage
 //                shared-memory ring, one thread issues tcgen05.mma
 //                (M=128, N=128, K=16) into a TMEM accumulator and commits
 //                each stage back to the producer through mbarriers, and the
-//                epilogue reads TMEM with tcgen05.ld. Optional split-K writes
-//                one FP32 partial per K range.
+//                epilogue reads TMEM with tcgen05.ld. Two CTAs share an SM,
+//                so one's epilogue overlaps the other's main loop; tiles run
+//                in grouped order for L2 reuse. Optional split-K writes one
+//                FP32 partial per K range.
 //   epilogue     sum of the split-K partials in a fixed order, bias,
 //                ReLU, BF16/FP32 outputs
 //   transpose, loss, ReLU backward, bias gradients, Adam
@@ -39,7 +41,7 @@ using bf16 = __nv_bfloat16;
 constexpr int BM = 128;
 constexpr int BN = 128;
 constexpr int BK = 64;                       // 64 BF16 = one 128-byte swizzle row
-constexpr int STAGES = 4;
+constexpr int STAGES = 3;                    // two CTAs per SM (shared memory)
 constexpr int GEMM_THREADS = 128;
 constexpr int STAGE_A_BYTES = BM * BK * 2;   // 16 KiB
 constexpr int STAGE_B_BYTES = BN * BK * 2;   // 16 KiB
@@ -155,7 +157,7 @@ struct GemmArgs {
     int* err;
 };
 
-__global__ void __launch_bounds__(GEMM_THREADS, 1)
+__global__ void __launch_bounds__(GEMM_THREADS, 2)
 gemm_tn(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
         GemmArgs a) {
     extern __shared__ uint8_t smem_raw[];
@@ -169,7 +171,15 @@ gemm_tn(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUten
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    // Grouped tile order: consecutive CTAs sweep kGroupM row tiles for each
+    // column tile, so the CTAs in flight share their A and B panels in L2.
+    constexpr int kGroupM = 16;
+    const int pid = blockIdx.x + blockIdx.y * gridDim.x;
+    const int per_group = kGroupM * gridDim.y;
+    const int first_m = (pid / per_group) * kGroupM;
+    const int group_m = min(static_cast<int>(gridDim.x) - first_m, kGroupM);
+    const int m0 = (first_m + (pid % per_group) % group_m) * BM;
+    const int n0 = ((pid % per_group) / group_m) * BN;
     const int total_kb = (a.K + BK - 1) / BK;
     const int kb0 = blockIdx.z * a.kblocks_per_split;
     const int kb1 = min(total_kb, kb0 + a.kblocks_per_split);
