@@ -531,13 +531,13 @@ def side_profile(args, opts, line):
         line["config"] = {"rows": p.lp.num_rows, "cols": p.lp.num_cols, "nnz": int(p.lp.nnz)}
         for prec, width in (("fp64", 1), ("mixed", 4)):
             tk = PdlpSolver(prec, vector_width=width).time_kernels_batch([p.lp], opts, reps=20)
-            out[prec] = _kernel_roofline(tk)
+            out[prec] = dict(_kernel_roofline(tk), padding={"at": tk["at_padding"], "a": tk["a_padding"]})
     else:
         sizes = g.uneven_batch_sizes(args.count)
         lps = [_planted_instance((i, sizes[i])).lp for i in range(args.count)]
         line["config"] = {"instances": args.count, "nnz": int(sum(q.nnz for q in lps))}
         tk = PdlpSolver(args.precision, vector_width=4, lane_elements=32).time_kernels_batch(lps, opts, reps=10)
-        out[args.precision] = _kernel_roofline(tk)
+        out[args.precision] = dict(_kernel_roofline(tk), padding={"at": tk["at_padding"], "a": tk["a_padding"]})
     line["profile"] = out
     return line
 
