@@ -17,6 +17,7 @@
 #include "control.cuh"
 #include "interleaved.cuh"
 
+#include <algorithm>
 #include <utility>
 
 namespace pdlpgpu {
@@ -999,20 +1000,51 @@ __global__ void k_il_family(Interleaved<T> il, FamSrc src, const double* __restr
 
 }  // namespace
 
-// Both trial kernels ask for the largest shared-memory carveout. Left to
+// Both trial kernels ask for one shared-memory carveout: the smallest that
+// holds, for either kernel, as many CTAs as its registers allow. Left to
 // itself the driver configures each kernel's SMs for its own needs (the dual
 // needs more shared memory than the primal), and an SM switches
 // configuration only once it is empty, so a kernel's CTAs could not take the
 // place of the previous kernel's finished CTAs on a busy SM: the
-// programmatic launch lost most of its overlap. Set on the current device at
-// setup, before any launch is captured.
+// programmatic launch lost most of its overlap. The smallest common carveout
+// leaves the rest of the SM's memory to L1, which the dual's decision reads
+// its control blocks through (measured on the flow stream, 256 slots: chunk
+// 5.83 ms with each kernel's own carveout, 5.52 with the largest, 5.35 with
+// this one). Set on the current device at setup, before any launch is
+// captured.
 template <class T, int V>
 void same_carveout() {
-    constexpr int kMaxShared = 100;   // percent
-    cudaFuncSetAttribute(k_il_primal<T, V, false>, cudaFuncAttributePreferredSharedMemoryCarveout, kMaxShared);
-    cudaFuncSetAttribute(k_il_primal<T, V, true>, cudaFuncAttributePreferredSharedMemoryCarveout, kMaxShared);
-    cudaFuncSetAttribute(k_il_dual<T, V, false>, cudaFuncAttributePreferredSharedMemoryCarveout, kMaxShared);
-    cudaFuncSetAttribute(k_il_dual<T, V, true>, cudaFuncAttributePreferredSharedMemoryCarveout, kMaxShared);
+    const void* const kernels[4] = {
+        reinterpret_cast<const void*>(k_il_primal<T, V, false>), reinterpret_cast<const void*>(k_il_primal<T, V, true>),
+        reinterpret_cast<const void*>(k_il_dual<T, V, false>), reinterpret_cast<const void*>(k_il_dual<T, V, true>)};
+    int dev = 0, smem_sm = 0, regs_sm = 0, reserved = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    size_t need = 0;
+    for (const void* k : kernels) {
+        cudaFuncAttributes a{};
+        if (cudaFuncGetAttributes(&a, k) != cudaSuccess || a.numRegs <= 0) continue;
+        const int blocks = regs_sm / (a.numRegs * kIlThreads);
+        need = std::max(need, static_cast<size_t>(blocks) * (a.sharedSizeBytes + static_cast<size_t>(reserved)));
+    }
+    // The driver takes the carveout as a preference and rounds it to the
+    // nearest shared-memory size an SM supports, so the request names the
+    // smallest supported size that holds `need` exactly.
+    constexpr int kSizesKb[] = {0, 8, 16, 32, 64, 100, 132, 164, 196, 228};
+    int percent = 100;
+    if (smem_sm > 0 && need > 0) {
+        for (int kb : kSizesKb) {
+            const size_t bytes = static_cast<size_t>(kb) * 1024;
+            if (bytes >= need && bytes <= static_cast<size_t>(smem_sm)) {
+                percent = static_cast<int>((100 * bytes + static_cast<size_t>(smem_sm) - 1) / static_cast<size_t>(smem_sm));
+                break;
+            }
+        }
+    }
+    for (const void* k : kernels) cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, percent);
+    cudaGetLastError();
 }
 
 template <class T, int V>
