@@ -113,6 +113,16 @@ enum {
     PDLPGPU_LAYOUT_INTERLEAVED = 2   /* vectors [line][instance]; a warp serves 32 instances */
 };
 
+/* Score of the restart test (RestartController::choose, restart_controller.cpp:8-63,
+ * keeps its thresholds and decisions; only the compared score changes). */
+enum {
+    PDLPGPU_RESTART_KKT = 0,         /* the reference's: the relative KKT error of each candidate */
+    PDLPGPU_RESTART_NORMALIZED_GAP = 1 /* the normalised duality gap of each candidate at the radius
+                                        * of its distance to the last restart point (weighted by
+                                        * the primal weight, in the scaled space of the iterations);
+                                        * pdlp_engine/README.md:226-233 names it as the missing metric */
+};
+
 /* Extensions with no counterpart in PdlpOptions. Zero means "default". */
 typedef struct pdlpgpu_ext_options {
     int32_t precision;             /* PDLPGPU_PRECISION_* */
@@ -127,7 +137,8 @@ typedef struct pdlpgpu_ext_options {
     int32_t layout;                /* sessions: PDLPGPU_LAYOUT_* */
     int32_t lane_instances;        /* interleaved layout: instances per lane, 1, 2 or 4 (0 = auto) */
     int32_t two_kernel_trials;     /* 1: never fuse a check interval's trials into one cluster launch */
-    int32_t reserved[4];
+    int32_t restart_metric;        /* PDLPGPU_RESTART_*: the score the restart test compares */
+    int32_t reserved[3];
 } pdlpgpu_ext_options;
 
 /* Optional warm start (this engine's extension; the reference starts from the

@@ -84,6 +84,21 @@ int32_t pdlpgpu_evaluate(const pdlpgpu_lp* lp, double infeasibility_tolerance,
                          const double* x, const double* y, const double* rx,
                          const double* ry, double* metrics, double* verdicts);
 
+/* No counterpart in the reference (pdlp_engine/README.md:226-233 names it as
+ * the restart metric still missing there): the normalised duality gap
+ * rho(r; z) of z = (x, y) for L(x, y) = c'x + y'Ax - h*(y) (h* the support
+ * function of the row bounds) over the box of x and the dual domain, in the
+ * ball ||(dx, dy)||_w^2 = w ||dx||^2 + ||dy||^2 / w <= r^2 whose radius r is
+ * the distance from z to (x_ref, y_ref). g = c + A'y [n] and a = A x [m] are
+ * given; bounds may be infinite. out[2] = {gap, radius}; the gap is +inf
+ * when the radius is zero. The device routine is the one the check stage
+ * uses for PDLPGPU_RESTART_NORMALIZED_GAP. Returns 0 on success. */
+int32_t pdlpgpu_normalized_gap(int32_t n, int32_t m, double weight, const double* x,
+                               const double* g, const double* x_lower, const double* x_upper,
+                               const double* x_ref, const double* y, const double* a,
+                               const double* r_lower, const double* r_upper, const double* y_ref,
+                               double* out);
+
 /* Layout statistics without a device (host only): slices, slots and real
  * entries of both sides, for the tuning in `ext` (NULL = autotune).
  * stats[8] = {a slices, a slots, a entries, at slices, at slots, at entries,

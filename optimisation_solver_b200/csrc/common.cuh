@@ -184,6 +184,8 @@ struct DeviceOptions {
     // every trial); indices past step_pow_entries compute them directly.
     const double* step_pow;
     int64_t step_pow_entries;
+    // 1: restarts compare normalised duality gaps instead of KKT errors.
+    int32_t ndg_restarts;
 };
 
 // Partial sums per elementwise CTA of a check (slot meaning depends on side).

@@ -461,6 +461,11 @@ bool Engine::prepare(const SolveSpec& spec) {
     plan.add(g_.count_dual, count_);
     plan.add(g_.count_check, count_);
     plan.add(d_active_, 2);
+    if (spec.ext.restart_metric == PDLPGPU_RESTART_NORMALIZED_GAP)
+        for (int k = 0; k < 2; ++k) {
+            plan.add(g_.ndg_g[k], N);
+            plan.add(g_.ndg_a[k], R);
+        }
     auto plan_work = [&](auto& w, int64_t Rn, int64_t Nn) {
         for (int k = 0; k < 2; ++k) {
             plan.add(w.X[k], Nn);
@@ -475,6 +480,10 @@ bool Engine::prepare(const SolveSpec& spec) {
     arena_bytes_ = plan.total();
     if (!check(cudaMalloc(&arena_, arena_bytes_), "cudaMalloc")) return false;
     plan.assign(arena_);
+    g_.rx64 = w64_.rx;
+    g_.ry64 = w64_.ry;
+    g_.rx32 = mixed_ ? w32_.rx : nullptr;
+    g_.ry32 = mixed_ ? w32_.ry : nullptr;
     if (!check(cudaMallocHost(&h_active_, 2 * sizeof(int32_t)), "cudaMallocHost")) return false;
     if (!check(cudaMemsetAsync(arena_, 0, arena_bytes_, stream_), "cudaMemset")) return false;
     mark("maps and arena");
@@ -634,6 +643,7 @@ bool Engine::prepare(const SolveSpec& spec) {
     dopt_.artificial = o.restart_artificial_fraction;
     dopt_.infeasibility_tol = o.infeasibility_tolerance;
     dopt_.time_limit = o.time_limit_seconds;
+    dopt_.ndg_restarts = spec.ext.restart_metric == PDLPGPU_RESTART_NORMALIZED_GAP ? 1 : 0;
     {
         // Step factors for every iteration index a solve can reach (main loop
         // and polishing), at most 2^20 of them (16 MiB).
@@ -843,6 +853,7 @@ void Engine::enqueue_check_stage(bool il_sync) {
     if (mixed_) launch_check_prep<float>(g_, w32_, dopt_, stream_);
     launch_check_prep<double>(g_, w64_, dopt_, stream_);
     launch_check_spmv(g_, dopt_, V, stream_);
+    launch_check_ndg(g_, dopt_, count_, stream_);
     if (mixed_) launch_check_apply<float>(g_, w32_, dopt_, stream_);
     launch_check_apply<double>(g_, w64_, dopt_, stream_);
     // Mixed: instances the check moves to the FP64 stage take their last
@@ -1375,6 +1386,7 @@ bool Engine::component_evaluate(const double* x, const double* y, const double* 
     if (!ok) return check(cudaErrorInvalidValue, "upload");
     launch_check_prep<double>(g_, w64_, dopt_, stream_);
     launch_check_spmv(g_, dopt_, V, stream_);
+    launch_check_ndg(g_, dopt_, count_, stream_);
     if (!check(cudaMemcpyAsync(&c, g_.ctl, sizeof(c), cudaMemcpyDeviceToHost, stream_), "download") ||
         !check(cudaStreamSynchronize(stream_), "evaluate"))
         return false;

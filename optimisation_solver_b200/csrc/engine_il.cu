@@ -86,7 +86,7 @@ int Engine::chunk_slots() const {
 }
 
 int Engine::check_stage_launches(bool il_sync) const {
-    return (mixed_ ? 8 : 5) + (il_sync && il_ ? 2 : 0);
+    return (mixed_ ? 8 : 5) + (il_sync && il_ ? 2 : 0) + (dopt_.ndg_restarts ? 1 : 0);
 }
 
 template <class T>

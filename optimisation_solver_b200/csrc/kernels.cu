@@ -27,6 +27,7 @@
 // atomic is the per-instance arrival counter.
 #include "control.cuh"
 #include "kernels.cuh"
+#include "ndg.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -883,9 +884,11 @@ __global__ void __launch_bounds__(kThreads) k_check_prep(Global g, Work<T> w, De
 // The decision of one check from its sums (pdlp_solver.cpp:239-476,
 // feasibility_polishing.cpp:107-141). C/R: column- and row-side elementwise
 // sums (kPrepSlots each), A3: row-pass sums, T6: column-pass sums.
+// `ndg`: with normalised-gap restarts at a main check, the gaps of the
+// current and average iterates (else null).
 __device__ __noinline__ void check_decide(const DeviceOptions& o, InstanceCtl& c, int32_t n_cols,
                                           const double* C, const double* R, const double* A3,
-                                          const double* T6) {
+                                          const double* T6, const double* ndg) {
 
     c.pending_avg = 0;
     const bool have_avg = check_have_avg(c, o);
@@ -935,7 +938,9 @@ __device__ __noinline__ void check_decide(const DeviceOptions& o, InstanceCtl& c
             c.need_refresh = 1;
         }
         store_best(c, start);
-        c.restart_baseline = start.kkt;
+        // A normalised gap needs a radius, which the starting point does not
+        // have yet: only the artificial test can trigger the first restart.
+        c.restart_baseline = o.ndg_restarts ? INFINITY : start.kkt;
         c.avg_weight = 0.0;
         c.have_avg_at_check = 0;
         if (is_optimal_best(c, o)) {
@@ -1013,7 +1018,8 @@ __device__ __noinline__ void check_decide(const DeviceOptions& o, InstanceCtl& c
         return;
     }
     double score;
-    const int choice = restart_choose(c, o, cur.kkt, avg.kkt, &score);
+    const int choice = ndg ? restart_choose(c, o, ndg[0], ndg[1], &score)
+                           : restart_choose(c, o, cur.kkt, avg.kkt, &score);
     if (choice != 0) {
         const bool from_avg = choice == 2 && have_avg;
         update_weight(c.omega, o, sqrt(from_avg ? C[6] : C[5]), sqrt(from_avg ? R[8] : R[7]));
@@ -1049,7 +1055,7 @@ __device__ __noinline__ void check_decide(const DeviceOptions& o, InstanceCtl& c
 }
 
 __device__ __noinline__ void check_control(const Global& g, const DeviceOptions& o, InstanceCtl& c,
-                              const InstanceInfo& inf) {
+                              const InstanceInfo& inf, const double* ndg) {
     // Column-side and row-side elementwise partials.
     double C[kPrepSlots], R[kPrepSlots], A3[3], T6[kCheckSlots];
     for (int q = 0; q < kPrepSlots; ++q) { C[q] = 0.0; R[q] = 0.0; }
@@ -1072,7 +1078,59 @@ __device__ __noinline__ void check_control(const Global& g, const DeviceOptions&
     const int at0 = g.a.num_ctas + inf.at_cta_begin, at1 = g.a.num_ctas + inf.at_cta_end;
     for (int q = 0; q < kCheckSlots; ++q) T6[q] = warp_range_sum(g.part_check, at0, at1, kCheckSlots, q);
     if (lane != 0) return;
-    check_decide(o, c, inf.n, C, R, A3, T6);
+    check_decide(o, c, inf.n, C, R, A3, T6, ndg);
+}
+
+// The candidate coordinates of a main check in the scaled space of the
+// iterations (x = x_o / cs, y = y_o / rs, c + A'y scaled by cs, A x by rs,
+// bounds scaled like the iterates), from what the check stored in original
+// coordinates; the restart point comes from the working arrays.
+struct CheckNdgCoord {
+    const Global* g;
+    int64_t col0, row0, n;
+    int which;    // 0 current, 1 average
+    bool fp32;    // restart point in the FP32 working arrays
+    __device__ NdgCoord operator()(int64_t k) const {
+        NdgCoord q;
+        if (k < n) {
+            const int64_t j = col0 + k;
+            const double cs = g->cs[j];
+            q.v = (which ? g->xa_o[j] : g->x_o[j]) / cs;
+            q.d = cs * g->ndg_g[which][j];
+            q.lo = g->xl_orig[j] / cs;
+            q.hi = g->xu_orig[j] / cs;
+            q.r = fp32 ? static_cast<double>(g->rx32[j]) : g->rx64[j];
+        } else {
+            const int64_t i = row0 + (k - n);
+            const double rs = g->rs[i];
+            q.v = (which ? g->ya_o[i] : g->y_o[i]) / rs;
+            q.d = rs * g->ndg_a[which][i];
+            q.lo = g->rl_orig[i] * rs;
+            q.hi = g->ru_orig[i] * rs;
+            q.r = fp32 ? static_cast<double>(g->ry32[i]) : g->ry64[i];
+        }
+        return q;
+    }
+};
+
+// Normalised gaps of the current and the average iterate (the same value
+// twice without an average), computed by the whole CTA; out[0..1] in shared
+// memory, valid after the CTA's next barrier.
+__device__ __noinline__ void check_ndg(const Global& g, const DeviceOptions& o, const InstanceCtl& c,
+                                       const InstanceInfo& inf, double* out) {
+    __shared__ double scratch[16 * 32];
+    const bool fp32 = o.mixed && !c.fp64_stage;
+    CheckNdgCoord q{&g, inf.col_off, inf.row_off, inf.n, 0, fp32};
+    const double cur = block_normalized_gap(inf.n, inf.m, c.omega, q, scratch, nullptr);
+    double avg = cur;
+    if (check_have_avg(c, o)) {
+        q.which = 1;
+        avg = block_normalized_gap(inf.n, inf.m, c.omega, q, scratch, nullptr);
+    }
+    if (threadIdx.x == 0) {
+        out[0] = cur;
+        out[1] = avg;
+    }
 }
 
 template <int V>
@@ -1086,6 +1144,7 @@ __global__ void __launch_bounds__(kThreads) k_check_spmv(Global g, DeviceOptions
     const bool have_avg = check_have_avg(c, o);
     const bool rays =
         (c.check_kind == kCheckMain || c.check_kind == kCheckEvaluate) && o.detect_infeasibility;
+    const bool ndg = o.ndg_restarts && o.restarts && c.check_kind == kCheckMain;
 
     double acc[kCheckSlots];
 #pragma unroll
@@ -1110,6 +1169,10 @@ __global__ void __launch_bounds__(kThreads) k_check_spmv(Global g, DeviceOptions
                             });
             if (lp.valid && lp.g == 0) {
                 const int64_t k = inf.row_off + lp.line;
+                if (ndg) {
+                    g.ndg_a[0][k] = sum[0];
+                    if (have_avg) g.ndg_a[1][k] = sum[1];
+                }
                 const double lo = g.rl_orig[k], hi = g.ru_orig[k];
                 const double e0 = sum[0] - smax(lo, smin(sum[0], hi));
                 acc[0] += e0 * e0;
@@ -1150,6 +1213,7 @@ __global__ void __launch_bounds__(kThreads) k_check_spmv(Global g, DeviceOptions
                 for (int which = 0; which < 2; ++which) {
                     if (which == 1 && !have_avg) break;
                     const double reduced = co + sum[which];
+                    if (ndg) g.ndg_g[which][k] = reduced;
                     double q = reduced;
                     if (!lo_f) q = smin(q, 0.0);
                     if (!hi_f) q = smax(q, 0.0);
@@ -1179,10 +1243,30 @@ __global__ void __launch_bounds__(kThreads) k_check_spmv(Global g, DeviceOptions
     }
     const int expected = (inf.a_cta_end - inf.a_cta_begin) + (inf.at_cta_end - inf.at_cta_begin);
     if (!arrive_last(g.count_check + cw.instance, expected)) return;
+    // With normalised-gap restarts, k_check_ndg takes the decision.
+    if (o.ndg_restarts) return;
     __shared__ DeviceOptions so;   // see k_dual
     if (threadIdx.x == 0) so = o;
     __syncthreads();
-    if (threadIdx.x < 32) check_control(g, so, c, inf);
+    if (threadIdx.x < 32) check_control(g, so, c, inf, nullptr);
+}
+
+// The check decision with normalised-gap restarts: one CTA per instance,
+// after k_check_spmv. At a main check the CTA first computes the two
+// candidates' normalised gaps from the products k_check_spmv stored.
+__global__ void __launch_bounds__(kThreads) k_check_ndg(Global g, DeviceOptions o) {
+    const int b = blockIdx.x;
+    InstanceCtl& c = g.ctl[b];
+    if (c.stage != kStageCheck || c.check_kind == kCheckTransition) return;
+    const InstanceInfo inf = g.info[b];
+    __shared__ DeviceOptions so;   // see k_dual
+    __shared__ double gaps[2];
+    if (threadIdx.x == 0) so = o;
+    __syncthreads();
+    const bool main = o.restarts && c.check_kind == kCheckMain;
+    if (main) check_ndg(g, so, c, inf, gaps);
+    __syncthreads();
+    if (threadIdx.x < 32) check_control(g, so, c, inf, main ? gaps : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -1868,6 +1952,10 @@ void launch_check_spmv(const Global& g, const DeviceOptions& o, int vw, cudaStre
         case 2: k_check_spmv<2><<<n, kThreads, 0, s>>>(g, o); break;
         default: k_check_spmv<1><<<n, kThreads, 0, s>>>(g, o); break;
     }
+}
+
+void launch_check_ndg(const Global& g, const DeviceOptions& o, int32_t count, cudaStream_t s) {
+    if (o.ndg_restarts && count > 0) k_check_ndg<<<count, kThreads, 0, s>>>(g, o);
 }
 
 template <class T>

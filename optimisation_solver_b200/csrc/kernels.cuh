@@ -87,6 +87,16 @@ struct Global {
     int32_t mixed;
     // Streams: when set, setup kernels act only on slots with slot_mask[b] != 0.
     const int32_t* slot_mask;
+    // Normalised-gap restarts (DeviceOptions::ndg_restarts): a main check's
+    // reduced costs c + A'y [column space] and row activities A x [row
+    // space] of the current (0) and average (1) iterates, original
+    // coordinates; and the restart point of each working precision.
+    double* ndg_g[2];
+    double* ndg_a[2];
+    const float* rx32;
+    const float* ry32;
+    const double* rx64;
+    const double* ry64;
 };
 
 // --- launches (kernels.cu). `vw` is the vector width (1, 2 or 4). ---------
@@ -111,6 +121,9 @@ constexpr int kFusedCtaThreads = 512;
 template <class T>
 void launch_check_prep(const Global& g, const Work<T>& w, const DeviceOptions& o, cudaStream_t s);
 void launch_check_spmv(const Global& g, const DeviceOptions& o, int vw, cudaStream_t s);
+// With normalised-gap restarts (o.ndg_restarts): the decision of each
+// instance at a check, after launch_check_spmv (one CTA per instance).
+void launch_check_ndg(const Global& g, const DeviceOptions& o, int32_t count, cudaStream_t s);
 template <class T>
 void launch_check_apply(const Global& g, const Work<T>& w, const DeviceOptions& o, cudaStream_t s);
 template <class T>

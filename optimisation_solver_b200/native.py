@@ -58,7 +58,8 @@ class ExtOptions(C.Structure):
                 ("fp32_stall_checks", C.c_int32), ("fp32_switch_factor", C.c_int32),
                 ("disable_graphs", C.c_int32), ("cta_slots", C.c_int32),
                 ("layout", C.c_int32), ("lane_instances", C.c_int32),
-                ("two_kernel_trials", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("two_kernel_trials", C.c_int32), ("restart_metric", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
 
 
 class WarmStart(C.Structure):
@@ -100,6 +101,7 @@ SIGNATURES = {
     "pdlpgpu_trial": (C.c_int32, [C.POINTER(Lp), C.c_int32] + [_dp] * 7 +
                       [C.c_double, C.c_double] + [_dp] * 4),
     "pdlpgpu_evaluate": (C.c_int32, [C.POINTER(Lp), C.c_double] + [_dp] * 6),
+    "pdlpgpu_normalized_gap": (C.c_int32, [C.c_int32, C.c_int32, C.c_double] + [_dp] * 10 + [_dp]),
     "pdlpgpu_trial_noalloc": (C.c_int32, [C.c_int32, C.c_int32] + [C.c_void_p] * 18 +
                               [C.c_double, C.c_double] + [C.c_void_p] * 5),
     "pdlpgpu_layout_stats": (C.c_int32, [C.POINTER(Lp), C.POINTER(ExtOptions), _i64p]),

@@ -203,6 +203,19 @@ def evaluate(problem: CompiledLp, x, y, rx=None, ry=None, infeasibility_toleranc
     return metrics, verdicts
 
 
+def normalized_gap(weight, x, g, x_lower, x_upper, x_ref, y, a, r_lower, r_upper, y_ref):
+    """The normalised duality gap of (x, y) on the device (pdlpgpu_normalized_gap):
+    g = c + A'y, a = A x, radius = the weighted distance to (x_ref, y_ref).
+    Returns (gap, radius)."""
+    arr = [np.ascontiguousarray(v, dtype=np.float64)
+           for v in (x, g, x_lower, x_upper, x_ref, y, a, r_lower, r_upper, y_ref)]
+    n, m = arr[0].size, arr[5].size
+    out = np.zeros(2)
+    _check(native.lib().pdlpgpu_normalized_gap(n, m, float(weight), *[native.ptr(v) for v in arr],
+                                               native.ptr(out)), "normalized_gap")
+    return float(out[0]), float(out[1])
+
+
 def layout_stats(problem: CompiledLp, lane_elements: int = 0, vector_width: int = 0,
                  precision: str = "fp64") -> dict:
     """Host-only statistics of the SELL-G layout (no device needed)."""
