@@ -566,6 +566,22 @@ def extras(args, session, graph, sup, cost, inputs, value, iters, solve, family,
                                "optimal_fraction": r64["optimal"] / sup.shape[0],
                                "warm_start": "cold" if args.cold else "learned",
                                "mixed_over_fp64": round(value / (sup.shape[0] / dt), 3)}
+    # The same instances with restarts on the normalised duality gap instead
+    # of the reference's KKT score (restart_metric=1; the statuses and the
+    # tolerance stay the reference's).
+    sg = Session(family, args.slots, options, precision=args.precision, device=device, restart_metric=1)
+    solve(sup[: args.batch], cost[: args.batch], warm=not args.cold, sess=sg)   # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rg, _ = solve(sup, cost, warm=not args.cold, sess=sg)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    sg.close()
+    out["gap_restarts"] = {"lps_per_s": round(sup.shape[0] / dt, 2),
+                           "mean_iterations": float(rg["iterations"].mean()),
+                           "optimal_fraction": rg["optimal"] / sup.shape[0],
+                           "max_relative_kkt": float(np.max(np.maximum.reduce(
+                               [rg["primal_residual"], rg["dual_residual"], rg["relative_gap"]])))}
     if not args.cold:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
