@@ -1094,16 +1094,16 @@ struct CheckNdgCoord {
         NdgCoord q;
         if (k < n) {
             const int64_t j = col0 + k;
-            const double cs = g->cs[j];
-            q.v = (which ? g->xa_o[j] : g->x_o[j]) / cs;
+            const double cs = g->cs[j], ics = 1.0 / cs;
+            q.v = (which ? g->xa_o[j] : g->x_o[j]) * ics;
             q.d = cs * g->ndg_g[which][j];
-            q.lo = g->xl_orig[j] / cs;
-            q.hi = g->xu_orig[j] / cs;
+            q.lo = g->xl_orig[j] * ics;
+            q.hi = g->xu_orig[j] * ics;
             q.r = fp32 ? static_cast<double>(g->rx32[j]) : g->rx64[j];
         } else {
             const int64_t i = row0 + (k - n);
             const double rs = g->rs[i];
-            q.v = (which ? g->ya_o[i] : g->y_o[i]) / rs;
+            q.v = (which ? g->ya_o[i] : g->y_o[i]) * (1.0 / rs);
             q.d = rs * g->ndg_a[which][i];
             q.lo = g->rl_orig[i] * rs;
             q.hi = g->ru_orig[i] * rs;

@@ -33,11 +33,12 @@ struct NdgCoord {
     double v, d, lo, hi, r;
 };
 
-// Primal coordinate: step from v at multiplier lam (lam <= 0: the box limit).
-__device__ __forceinline__ double ndg_primal_step(const NdgCoord& q, double lam, double w) {
+// Primal coordinate: step from v at multiplier lam (lam <= 0: the box limit);
+// `inv` = 1 / (lam w), computed once per multiplier.
+__device__ __forceinline__ double ndg_primal_step(const NdgCoord& q, double lam, double inv) {
     double s;
     if (lam > 0.0) {
-        s = -q.d / (lam * w);
+        s = -q.d * inv;
     } else {
         s = q.d < 0.0 ? INFINITY : (q.d > 0.0 ? -INFINITY : 0.0);
     }
@@ -50,12 +51,13 @@ __device__ __forceinline__ double ndg_support(double v, double lo, double hi) {
     return v > 0.0 ? hi * v : (v < 0.0 ? lo * v : 0.0);
 }
 
-// Dual coordinate: maximiser of (yh - v) d - h*(yh) - lam / (2 w) (yh - v)^2.
-__device__ __forceinline__ double ndg_dual_point(const NdgCoord& q, double lam, double w) {
+// Dual coordinate: maximiser of (yh - v) d - h*(yh) - lam / (2 w) (yh - v)^2;
+// `wl` = w / lam.
+__device__ __forceinline__ double ndg_dual_point(const NdgCoord& q, double lam, double wl) {
     const bool hi_f = isfinite(q.hi), lo_f = isfinite(q.lo);
     if (lam > 0.0) {
-        const double up = q.v + (w / lam) * (q.d - q.hi);
-        const double dn = q.v + (w / lam) * (q.d - q.lo);
+        const double up = q.v + wl * (q.d - q.hi);
+        const double dn = q.v + wl * (q.d - q.lo);
         if (hi_f && up > 0.0) return up;
         if (lo_f && dn < 0.0) return dn;
         return 0.0;
@@ -101,24 +103,24 @@ __device__ double block_normalized_gap(int64_t n, int64_t m, double w, Coord coo
     // Pass 1: the radius, the distance at lam = 1 (clipped) and without the
     // box (unclipped, an upper bound of dist(lam) * lam).
     double s3[3] = {0.0, 0.0, 0.0};
+    const double iw = 1.0 / w;
     for (int64_t k = threadIdx.x; k < total; k += blockDim.x) {
         const NdgCoord q = coord(k);
         if (k < n) {
             const double e = q.v - q.r;
             s3[0] += w * e * e;
-            const double st = ndg_primal_step(q, 1.0, w);
+            const double st = ndg_primal_step(q, 1.0, iw);
             s3[1] += w * st * st;
-            const double u = q.d / w;
-            s3[2] += w * u * u;
+            s3[2] += q.d * q.d * iw;
         } else {
             const double e = q.v - q.r;
-            s3[0] += e * e / w;
+            s3[0] += e * e * iw;
             const double st = ndg_dual_point(q, 1.0, w) - q.v;
-            s3[1] += st * st / w;
+            s3[1] += st * st * iw;
             const double up = isfinite(q.hi) ? w * (q.d - q.hi) : 0.0;
             const double dn = isfinite(q.lo) ? w * (q.d - q.lo) : 0.0;
             const double u = fabs(up) > fabs(dn) ? up : dn;
-            s3[2] += u * u / w;
+            s3[2] += u * u * iw;
         }
     }
     {
@@ -152,15 +154,16 @@ __device__ double block_normalized_gap(int64_t n, int64_t m, double w, Coord coo
             double v1[K];
 #pragma unroll
             for (int k = 0; k < K; ++k) v1[k] = 0.0;
+            const double inv = 1.0 / (lo * w), wl = w / lo;
             for (int64_t k = threadIdx.x; k < total; k += blockDim.x) {
                 const NdgCoord q = coord(k);
                 double st;
                 if (k < n) {
-                    st = ndg_primal_step(q, lo, w);
+                    st = ndg_primal_step(q, lo, inv);
                     v1[0] += w * st * st;
                 } else {
-                    st = ndg_dual_point(q, lo, w) - q.v;
-                    v1[0] += st * st / w;
+                    st = ndg_dual_point(q, lo, wl) - q.v;
+                    v1[0] += st * st * iw;
                 }
             }
             ndg_block_sum<K>(v1, scratch);
@@ -171,22 +174,36 @@ __device__ double block_normalized_gap(int64_t n, int64_t m, double w, Coord coo
         } else {
             for (int pass = 0; pass < kPasses && hi > lo * (1.0 + 1e-12); ++pass) {
                 const double ratio = log(hi / lo);
+                // Per multiplier: lam, 1 / (lam w) and w / lam (no division in
+                // the coordinate loop).
+                __shared__ double lks[3][K];
+                if (threadIdx.x < K) {
+                    const double l = lo * exp(ratio * static_cast<double>(threadIdx.x + 1) /
+                                              static_cast<double>(K + 1));
+                    lks[0][threadIdx.x] = l;
+                    lks[1][threadIdx.x] = 1.0 / (l * w);
+                    lks[2][threadIdx.x] = w / l;
+                }
+                __syncthreads();
                 double lk[K], v[K];
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
-                    lk[k] = lo * exp(ratio * static_cast<double>(k + 1) / static_cast<double>(K + 1));
+                    lk[k] = lks[0][k];
                     v[k] = 0.0;
                 }
                 for (int64_t j = threadIdx.x; j < total; j += blockDim.x) {
                     const NdgCoord q = coord(j);
+                    if (j < n) {
 #pragma unroll
-                    for (int k = 0; k < K; ++k) {
-                        if (j < n) {
-                            const double st = ndg_primal_step(q, lk[k], w);
+                        for (int k = 0; k < K; ++k) {
+                            const double st = ndg_primal_step(q, lk[k], lks[1][k]);
                             v[k] += w * st * st;
-                        } else {
-                            const double st = ndg_dual_point(q, lk[k], w) - q.v;
-                            v[k] += st * st / w;
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < K; ++k) {
+                            const double st = ndg_dual_point(q, lk[k], lks[2][k]) - q.v;
+                            v[k] += st * st * iw;
                         }
                     }
                 }
@@ -211,13 +228,14 @@ __device__ double block_normalized_gap(int64_t n, int64_t m, double w, Coord coo
     double ov[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) ov[k] = 0.0;
+    const double inv = lam > 0.0 ? 1.0 / (lam * w) : 0.0, wl = lam > 0.0 ? w / lam : 0.0;
     for (int64_t k = threadIdx.x; k < total; k += blockDim.x) {
         const NdgCoord q = coord(k);
         if (k < n) {
-            const double st = ndg_primal_step(q, lam, w);
+            const double st = ndg_primal_step(q, lam, inv);
             if (st != 0.0) ov[0] += -q.d * st;
         } else {
-            const double yh = ndg_dual_point(q, lam, w);
+            const double yh = ndg_dual_point(q, lam, wl);
             ov[0] += (yh - q.v) * q.d - ndg_support(yh, q.lo, q.hi) + ndg_support(q.v, q.lo, q.hi);
         }
     }
