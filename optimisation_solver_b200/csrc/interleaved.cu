@@ -2,15 +2,16 @@
 // shared-matrix session, and the transposes between it and the per-instance
 // layout the checks use.
 //
-// Per trial (pdlp_engine/src/pdhg_kernel.cpp:47-187), lane b of a warp is
-// instance group * 32 + b and the warp walks one line:
+// Per trial (pdlp_engine/src/pdhg_kernel.cpp:47-187), lane l of a warp holds
+// instances group * G + l * V + v (V = 1, 2 or 4 per lane, G = 32 V) and the
+// warp walks one line:
 //   k_il_primal  column j: g = c + A'y, x' = clip(x - (eta/omega) tau g),
 //                sum dx^2/tau; the owed iterate-average update of x
 //                (iterate_average.cpp:40-82)
 //   k_il_dual    row i: A x', extrapolation 2Ax' - Ax, dual prox, sum
 //                dy^2/sigma and dy'(A dx); the owed average update of y; then,
 //                in the last CTA of each group, the linesearch decision and
-//                commit of its 32 instances (trial_control, one lane each).
+//                commit of its G instances (trial_control, one thread each).
 // Sums are per lane: each CTA adds its warps' values in warp order and
 // writes one partial per lane; the deciding CTA adds the partials in CTA
 // order, so a run is bitwise reproducible and needs no atomics on data.

@@ -61,7 +61,10 @@ def _warm_struct(warm, keep):
 
 class PdlpSolver:
     """Device PDLP solver. ``precision`` is "fp64" (the reference's
-    arithmetic) or "mixed"; ``device`` is the CUDA ordinal."""
+    arithmetic) or "mixed"; ``device`` is the CUDA ordinal. Further keywords
+    are fields of ``pdlpgpu_ext_options`` (include/pdlpgpu.h), e.g.
+    ``lane_elements``, ``vector_width``, ``two_kernel_trials=1`` or
+    ``restart_metric=1`` (restarts on the normalised duality gap)."""
 
     def __init__(self, precision: str = "fp64", device: int = 0, **tuning):
         if precision not in _PRECISIONS:
