@@ -894,18 +894,25 @@ void Engine::choose_fused() {
     for (int b = 0; b < count_; ++b)
         entries = std::max({entries, info_[static_cast<size_t>(b)].a_cta_end - info_[static_cast<size_t>(b)].a_cta_begin,
                             info_[static_cast<size_t>(b)].at_cta_end - info_[static_cast<size_t>(b)].at_cta_begin});
-    const int groups_per_cta = kFusedCtaThreads / kThreads;
+    // A warp of the fused kernel sums an entry's slices one after another;
+    // that equals the two-kernel path's block sum (one slice per warp) only
+    // while no entry has more slices than a CTA has warps.
+    for (const auto* side : {&a_ctas_, &at_ctas_})
+        for (const CtaWork& cw : *side)
+            if (cw.slice_end - cw.slice_begin > kThreads / 32) return;
+    const int warps_per_cta = kFusedCtaThreads / 32;
     const int V = tuning_.vector_width;
     auto resident = [&](int cluster) {
         return mixed_ ? std::min(fused_max_clusters<float>(V, cluster), fused_max_clusters<double>(V, cluster))
                       : fused_max_clusters<double>(V, cluster);
     };
-    // The smallest cluster that serves every entry in one round, up to 16
-    // CTAs (8 where the device cannot hold 16), then at most four rounds.
+    // The smallest cluster whose warps serve every entry in one round, up to
+    // 16 CTAs (8 where the device cannot hold 16); the kernel's partial-sum
+    // arrays hold at most kFusedMaxEntries entries.
     int cluster = 1;
-    while (cluster < 16 && cluster * groups_per_cta < entries) cluster *= 2;
+    while (cluster < 16 && cluster * warps_per_cta < entries) cluster *= 2;
     if (cluster == 16 && resident(16) <= 0) cluster = 8;
-    if (entries > 4 * cluster * groups_per_cta || resident(cluster) <= 0) return;
+    if (entries > kFusedMaxEntriesHost || resident(cluster) <= 0) return;
     fused_cluster_ = cluster;
 }
 

@@ -459,9 +459,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_dual(Global g, Work<T> w, Devic
 
 // ---------------------------------------------------------------------------
 // Fused trials of small LPs: one thread-block cluster per instance runs the
-// trials of a check interval in one launch. CTA rank r of the cluster serves
-// the instance's CTA-map entries r * kFusedGroups + q, stepping by the
-// cluster's group count, with its group q of 256 threads; per trial:
+// trials of a check interval in one launch. Warp q of CTA rank r serves the
+// instance's CTA-map entries r * kFusedWarps + q, stepping by the cluster's
+// warp count (an entry's slices one after another); per trial:
 //   primal half of every entry (k_primal's arithmetic, its partial per entry)
 //   cluster barrier
 //   dual half of every entry (k_dual's arithmetic)
@@ -478,6 +478,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_dual(Global g, Work<T> w, Devic
 // ---------------------------------------------------------------------------
 constexpr int kFusedGroups = 2;   // 512 threads: up to 128 registers each
 constexpr int kFusedThreads = kFusedGroups * kThreads;
+constexpr int kFusedWarps = kFusedThreads / 32;
 
 // Every thread of every CTA of the cluster; the warp is reconverged first
 // (the decision runs in one thread of rank 0's first warp just before).
@@ -501,26 +502,13 @@ __device__ __forceinline__ uint32_t cluster_size() {
 // block_sum over one 256-thread group (its warps added in warp order, as
 // block_sum adds a CTA's); the result is valid in the group's thread 0.
 // Named barrier 1 + group; a second barrier frees `red` for the next call.
+// The lanes' values of one warp added by the butterfly of block_sum's first
+// stage (every lane gets the sum).
 template <int NQ>
-__device__ __forceinline__ void group_sum(double (&v)[NQ], double (*red)[kWarps], int group, int lt) {
-    const int lane = lt & 31, warp = lt >> 5;
+__device__ __forceinline__ void warp_sum(double (&v)[NQ]) {
 #pragma unroll
     for (int q = 0; q < NQ; ++q)
         for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(kFull, v[q], o);
-    if (lane == 0) {
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) red[q][warp] = v[q];
-    }
-    asm volatile("bar.sync %0, %1;" ::"r"(1 + group), "r"(kThreads) : "memory");
-    if (lt == 0) {
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-            double t = 0.0;
-            for (int w = 0; w < kWarps; ++w) t += red[q][w];
-            v[q] = t;
-        }
-    }
-    asm volatile("bar.sync %0, %1;" ::"r"(1 + group), "r"(kThreads) : "memory");
 }
 
 struct FusedCtl {
@@ -666,7 +654,8 @@ __device__ __forceinline__ void fused_snapshot(const InstanceCtl& c, FusedCtl& f
     f.frac = c.avg_frac;
 }
 
-constexpr int kFusedMaxEntries = 4 * 16 * kFusedGroups;   // four rounds of the largest cluster
+constexpr int kFusedMaxEntries = kFusedMaxEntriesHost;
+static_assert(kFusedThreads == kFusedCtaThreads, "the engine sizes clusters by this CTA size");
 
 template <class T, int V>
 __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w, DeviceOptions o,
@@ -679,17 +668,17 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
     // memory when the launch ends.
     __shared__ DeviceOptions so;
     __shared__ FusedCtl f;
-    __shared__ double red[kFusedGroups][2][kWarps];
     __shared__ alignas(16) InstanceCtl sctl;
     __shared__ double part_p[kFusedMaxEntries];
     __shared__ double part_d[2 * kFusedMaxEntries];
     const uint32_t C = cluster_size(), rank = cluster_rank();
     const int b = static_cast<int>(blockIdx.x / C);
-    const int group = threadIdx.x / kThreads, lt = threadIdx.x % kThreads;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     InstanceCtl* cp = g.ctl + b;
     const InstanceInfo inf = g.info[b];
-    const int stride = static_cast<int>(C) * kFusedGroups;
-    const int slot = static_cast<int>(rank) * kFusedGroups + group;
+    // One warp per CTA-map entry: entry e goes to warp e mod (cluster warps).
+    const int stride = static_cast<int>(C) * kFusedWarps;
+    const int slot = static_cast<int>(rank) * kFusedWarps + warp;
     constexpr bool kFp64 = sizeof(T) == 8;
     if (threadIdx.x == 0) so = o;
     if (rank == 0) {
@@ -714,20 +703,36 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
         }
         __syncthreads();
         if (!f.active) break;
+        // An entry's slices one after another in one warp, each reduced over
+        // its lanes and added in slice order: with at most kWarps slices per
+        // entry (choose_fused), k_primal's block sum of one slice per warp.
         for (int e = inf.at_cta_begin + slot; e < inf.at_cta_end; e += stride) {
-            double moved[1] = {fused_primal<T, V>(g, w, g.at.ctas[e], inf, f, lt)};
-            group_sum<1>(moved, red[group], group, lt);
-            if (lt == 0) st_cluster(pp_addr + 8u * static_cast<uint32_t>(e - inf.at_cta_begin), moved[0]);
+            const CtaWork cw = g.at.ctas[e];
+            double total = 0.0;
+            for (int s = cw.slice_begin; s < cw.slice_end; ++s) {
+                const CtaWork one{cw.instance, s, s + 1, cw.pad};
+                double v[1] = {fused_primal<T, V>(g, w, one, inf, f, lane)};
+                warp_sum<1>(v);
+                total += v[0];
+            }
+            if (lane == 0) st_cluster(pp_addr + 8u * static_cast<uint32_t>(e - inf.at_cta_begin), total);
         }
         cluster_sync_all();
         for (int e = inf.a_cta_begin + slot; e < inf.a_cta_end; e += stride) {
-            double r2[2] = {0.0, 0.0};
-            fused_dual<T, V>(g, w, g.a.ctas[e], inf, f, lt, r2);
-            group_sum<2>(r2, red[group], group, lt);
-            if (lt == 0) {
+            const CtaWork cw = g.a.ctas[e];
+            double total[2] = {0.0, 0.0};
+            for (int s = cw.slice_begin; s < cw.slice_end; ++s) {
+                const CtaWork one{cw.instance, s, s + 1, cw.pad};
+                double r2[2] = {0.0, 0.0};
+                fused_dual<T, V>(g, w, one, inf, f, lane, r2);
+                warp_sum<2>(r2);
+                total[0] += r2[0];
+                total[1] += r2[1];
+            }
+            if (lane == 0) {
                 const uint32_t q = 16u * static_cast<uint32_t>(e - inf.a_cta_begin);
-                st_cluster(pd_addr + q, r2[0]);
-                st_cluster(pd_addr + q + 8u, r2[1]);
+                st_cluster(pd_addr + q, total[0]);
+                st_cluster(pd_addr + q + 8u, total[1]);
             }
         }
         cluster_sync_all();
