@@ -118,8 +118,9 @@ cudaError_t launch_fused(const Global& g, const Work<T>& w, const DeviceOptions&
 template <class T>
 int fused_max_clusters(int vw, int cluster);
 constexpr int kFusedCtaThreads = 512;
-// Entries per instance side the fused kernel's partial-sum arrays hold.
-constexpr int kFusedMaxEntriesHost = 128;
+// Entries per instance side the fused kernel's partial-sum arrays hold (four
+// rounds of the largest cluster's warps).
+constexpr int kFusedMaxEntriesHost = 1024;
 template <class T>
 void launch_check_prep(const Global& g, const Work<T>& w, const DeviceOptions& o, cudaStream_t s);
 void launch_check_spmv(const Global& g, const DeviceOptions& o, int vw, cudaStream_t s);
