@@ -32,16 +32,21 @@ __device__ __forceinline__ double clampd(double v, double lo, double hi) {
 template <class T> __device__ __forceinline__ T smin(T a, T b) { return b < a ? b : a; }
 template <class T> __device__ __forceinline__ T smax(T a, T b) { return a < b ? b : a; }
 
+// `factors`, when given, holds step_pow[2k] and step_pow[2k + 1] of this
+// iteration index, loaded by the caller ahead of the decision.
 __device__ inline bool evaluate_step(double& eta, double omega, double eta_max,
                                      const DeviceOptions& o, double pmove, double dmove,
-                                     double inter, int64_t iteration) {
+                                     double inter, int64_t iteration, const double* factors = nullptr) {
     const double movement = omega * pmove + dmove / omega;
     const double coupling = fabs(inter);
     double limit = INFINITY;
     if (coupling > 0.0 && movement > 0.0) limit = movement / (2.0 * coupling);
     const double index = static_cast<double>(iteration) + 2.0;
     double p3, p6;
-    if (iteration >= 0 && iteration < o.step_pow_entries) {
+    if (factors) {
+        p3 = factors[0];
+        p6 = factors[1];
+    } else if (iteration >= 0 && iteration < o.step_pow_entries) {
         p3 = o.step_pow[2 * iteration];
         p6 = o.step_pow[2 * iteration + 1];
     } else {
@@ -200,8 +205,11 @@ __device__ __forceinline__ void copy_ctl_warp(InstanceCtl* dst, const InstanceCt
 
 // After the two halves of one trial: finiteness test, linesearch decision,
 // commit, averaging and the check boundary.
+// `factors`: the linesearch's step factors of the trial's iteration index
+// (evaluate_step), or null to read them from the options' table.
 inline __device__ __noinline__ void trial_control(InstanceCtl& c, const DeviceOptions& o, double pmove,
-                                     double dmove, double inter, int32_t n_cols) {
+                                     double dmove, double inter, int32_t n_cols,
+                                     const double* factors = nullptr) {
     c.pending_avg = 0;
     c.dbg[0] = pmove;
     c.dbg[1] = dmove;
@@ -217,14 +225,14 @@ inline __device__ __noinline__ void trial_control(InstanceCtl& c, const DeviceOp
     bool accept;
     if (!polishing) {
         accept = !o.adaptive ||
-                 evaluate_step(c.eta, c.omega, c.eta_max, o, pmove, dmove, inter, c.iteration);
+                 evaluate_step(c.eta, c.omega, c.eta_max, o, pmove, dmove, inter, c.iteration, factors);
         c.trial_eta = c.eta;
         c.trial_omega = c.omega;
     } else if (!o.adaptive) {
         accept = true;
     } else {
         accept = evaluate_step(c.ctl_eta, c.ctl_omega, c.eta_max, o, pmove, dmove, inter,
-                               c.polish_iteration);
+                               c.polish_iteration, factors);
         c.trial_eta = c.ctl_eta;
     }
     if (!accept) {

@@ -885,35 +885,77 @@ int Engine::timed_position(int k, int slots) const {
 
 // Small instances run the trials of a check interval in one cluster launch
 // per precision (k_fused) instead of two launches per trial slot: up to 16
-// instances whose CTA maps take at most four rounds of a cluster's 2-group
-// CTAs, when the device can hold such a cluster.
+// instances whose slices' warp sums fit a CTA's shared memory, when the
+// device can hold such a cluster. When the cluster has a warp for every
+// slice and the warps' slices fit beside the sums, the slices are staged in
+// shared memory for the launch.
 void Engine::choose_fused() {
     fused_cluster_ = 0;
+    fused_shape_ = FusedShape{};
     if (il_ || spec_.ext.two_kernel_trials == 1 || count_ <= 0 || count_ > 16) return;
-    int entries = 0;
-    for (int b = 0; b < count_; ++b)
-        entries = std::max({entries, info_[static_cast<size_t>(b)].a_cta_end - info_[static_cast<size_t>(b)].a_cta_begin,
-                            info_[static_cast<size_t>(b)].at_cta_end - info_[static_cast<size_t>(b)].at_cta_begin});
-    // A warp of the fused kernel sums an entry's slices one after another;
-    // that equals the two-kernel path's block sum (one slice per warp) only
-    // while no entry has more slices than a CTA has warps.
+    // The fused kernel adds an entry's slice sums in slice order; that
+    // equals the two-kernel path's block sum (one slice per warp, warps in
+    // order) only while no entry has more slices than a CTA has warps.
     for (const auto* side : {&a_ctas_, &at_ctas_})
         for (const CtaWork& cw : *side)
             if (cw.slice_end - cw.slice_begin > kThreads / 32) return;
+    // An instance's slices are contiguous in its CTA map.
+    auto first = [](const std::vector<CtaWork>& side, int e0) { return side[static_cast<size_t>(e0)].slice_begin; };
+    auto last = [](const std::vector<CtaWork>& side, int e1) { return side[static_cast<size_t>(e1 - 1)].slice_end; };
+    FusedShape sh{};
+    for (int b = 0; b < count_; ++b) {
+        const InstanceInfo& inf = info_[static_cast<size_t>(b)];
+        sh.slices_p = std::max(sh.slices_p, last(at_ctas_, inf.at_cta_end) - first(at_ctas_, inf.at_cta_begin));
+        sh.slices_d = std::max(sh.slices_d, last(a_ctas_, inf.a_cta_end) - first(a_ctas_, inf.a_cta_begin));
+        sh.entries_p = std::max(sh.entries_p, inf.at_cta_end - inf.at_cta_begin);
+        sh.entries_d = std::max(sh.entries_d, inf.a_cta_end - inf.a_cta_begin);
+    }
+    if (fused_smem_bytes(sh) > kFusedMaxSmemHost) return;
     const int warps_per_cta = kFusedCtaThreads / 32;
     const int V = tuning_.vector_width;
-    auto resident = [&](int cluster) {
-        return mixed_ ? std::min(fused_max_clusters<float>(V, cluster), fused_max_clusters<double>(V, cluster))
-                      : fused_max_clusters<double>(V, cluster);
+    auto resident = [&](int cluster, const FusedShape& f) {
+        return mixed_ ? std::min(fused_max_clusters<float>(V, cluster, f), fused_max_clusters<double>(V, cluster, f))
+                      : fused_max_clusters<double>(V, cluster, f);
     };
-    // The smallest cluster whose warps serve every entry in one round, up to
-    // 16 CTAs (8 where the device cannot hold 16); the kernel's partial-sum
-    // arrays hold at most kFusedMaxEntries entries.
+    // The smallest cluster with a warp for every slice, up to 16 CTAs (8
+    // where the device cannot hold 16).
     int cluster = 1;
-    while (cluster < 16 && cluster * warps_per_cta < entries) cluster *= 2;
-    if (cluster == 16 && resident(16) <= 0) cluster = 8;
-    if (entries > kFusedMaxEntriesHost || resident(cluster) <= 0) return;
+    while (cluster < 16 && cluster * warps_per_cta < std::max(sh.slices_p, sh.slices_d)) cluster *= 2;
+    if (cluster == 16 && resident(16, sh) <= 0) cluster = 8;
+    if (resident(cluster, sh) <= 0) return;
+    if (cluster * warps_per_cta >= std::max(sh.slices_p, sh.slices_d)) {
+        // Staging: CTA rank r's warp q takes slice r * 16 + q of each side;
+        // its bytes at the FP64 element size (the larger of the two stages).
+        int64_t stage = 0;
+        for (int b = 0; b < count_; ++b) {
+            const InstanceInfo& inf = info_[static_cast<size_t>(b)];
+            const MatrixLayout& L = layouts_[spec_.shared_matrix ? 0 : b];
+            const int ps0 = first(at_ctas_, inf.at_cta_begin) - inf.at_slice_base;
+            const int ps1 = last(at_ctas_, inf.at_cta_end) - inf.at_slice_base;
+            const int ds0 = first(a_ctas_, inf.a_cta_begin) - inf.a_slice_base;
+            const int ds1 = last(a_ctas_, inf.a_cta_end) - inf.a_slice_base;
+            for (int r = 0; r < cluster; ++r) {
+                int64_t cta = 0;
+                for (int q = 0; q < warps_per_cta; ++q) {
+                    const int k = r * warps_per_cta + q;
+                    if (ps0 + k < ps1)
+                        cta += fused_slice_bytes(L.at.slices[static_cast<size_t>(ps0 + k)].steps, kFusedPrimalConsts,
+                                                 static_cast<int>(sizeof(double)));
+                    if (ds0 + k < ds1)
+                        cta += fused_slice_bytes(L.a.slices[static_cast<size_t>(ds0 + k)].steps, kFusedDualConsts,
+                                                 static_cast<int>(sizeof(double)));
+                }
+                stage = std::max(stage, cta);
+            }
+        }
+        FusedShape staged = sh;
+        staged.stage_bytes = static_cast<int32_t>(std::min<int64_t>(stage, INT32_MAX));
+        // Never zero when staged (the kernel tells the two modes apart by it).
+        staged.stage_bytes = std::max(staged.stage_bytes, 16);
+        if (fused_smem_bytes(staged) <= kFusedMaxSmemHost && resident(cluster, staged) > 0) sh = staged;
+    }
     fused_cluster_ = cluster;
+    fused_shape_ = sh;
 }
 
 void Engine::enqueue_chunk(int slots, bool fp64_stage) {
@@ -921,11 +963,12 @@ void Engine::enqueue_chunk(int slots, bool fp64_stage) {
         // One launch runs every instance's trials of the interval.
         const int V = tuning_.vector_width;
         record_timing(0);
-        if (mixed_) launch_fused<float>(g_, w32_, dopt_, V, count_, fused_cluster_, slots, stream_);
-        else launch_fused<double>(g_, w64_, dopt_, V, count_, fused_cluster_, slots, stream_);
+        const FusedShape& sh = fused_shape_;
+        if (mixed_) launch_fused<float>(g_, w32_, dopt_, V, count_, fused_cluster_, slots, sh, stream_);
+        else launch_fused<double>(g_, w64_, dopt_, V, count_, fused_cluster_, slots, sh, stream_);
         launches_ += 1;
         if (mixed_ && fp64_stage) {
-            launch_fused<double>(g_, w64_, dopt_, V, count_, fused_cluster_, slots, stream_);
+            launch_fused<double>(g_, w64_, dopt_, V, count_, fused_cluster_, slots, sh, stream_);
             launches_ += 1;
         }
         record_timing(1);

@@ -196,6 +196,7 @@ private:
     // kernels per trial slot. Chosen by choose_fused() for one-LP solves and
     // small batches.
     int fused_cluster_ = 0;
+    FusedShape fused_shape_{};   // shared memory of the fused launch
     void choose_fused();
     Interleaved<float> il32_{};
     Interleaved<double> il64_{};

@@ -460,13 +460,15 @@ __global__ void __launch_bounds__(kThreads, 4) k_dual(Global g, Work<T> w, Devic
 // ---------------------------------------------------------------------------
 // Fused trials of small LPs: one thread-block cluster per instance runs the
 // trials of a check interval in one launch. Warp q of CTA rank r serves the
-// instance's CTA-map entries r * kFusedWarps + q, stepping by the cluster's
-// warp count (an entry's slices one after another); per trial:
-//   primal half of every entry (k_primal's arithmetic, its partial per entry)
+// instance's slices r * kFusedWarps + q, stepping by the cluster's warp count;
+// per trial:
+//   primal half of every slice (k_primal's arithmetic, its warp sum per slice)
 //   cluster barrier
-//   dual half of every entry (k_dual's arithmetic)
+//   dual half of every slice (k_dual's arithmetic)
 //   cluster barrier
-//   rank 0: the three sums in k_dual's fixed order and trial_control
+//   rank 0: each CTA-map entry's slice sums added in slice order (k_primal's
+//   and k_dual's block sums: one slice per warp, warps in order), then the
+//   entries' three sums in k_dual's fixed order and trial_control
 //   cluster barrier
 // so an instance's results are the two-kernel path's bit for bit, without a
 // launch, an arrival counter or a trip through the decision's dependent loads
@@ -633,17 +635,6 @@ __device__ __forceinline__ uint32_t rank0_addr(const void* local) {
 __device__ __forceinline__ void st_cluster(uint32_t addr, double v) {
     asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v) : "memory");
 }
-__device__ __forceinline__ double ld_cluster_f64(uint32_t addr) {
-    double v;
-    asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(addr) : "memory");
-    return v;
-}
-__device__ __forceinline__ int ld_cluster_i32(uint32_t addr) {
-    int v;
-    asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
-    return v;
-}
-
 // The next trial's snapshot of an instance's control block.
 __device__ __forceinline__ void fused_snapshot(const InstanceCtl& c, FusedCtl& f, bool fp64) {
     f.active = c.phase != kPhaseDone && c.stage == kStageTrial && (c.fp64_stage != 0) == fp64;
@@ -654,103 +645,365 @@ __device__ __forceinline__ void fused_snapshot(const InstanceCtl& c, FusedCtl& f
     f.frac = c.avg_frac;
 }
 
-constexpr int kFusedMaxEntries = kFusedMaxEntriesHost;
 static_assert(kFusedThreads == kFusedCtaThreads, "the engine sizes clusters by this CTA size");
+
+// Distributed shared memory of rank `r`: the address of `local` there, and
+// stores of the snapshot's fields.
+__device__ __forceinline__ uint32_t rank_addr(const void* local, uint32_t r) {
+    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(local));
+    uint32_t out;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(a), "r"(r));
+    return out;
+}
+__device__ __forceinline__ void st_cluster_i32(uint32_t addr, int v) {
+    asm volatile("st.shared::cluster.s32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+// Rank 0's thread 0 writes the next trial's snapshot into every other CTA's
+// copy of `f`; the cluster barrier that follows publishes it.
+__device__ __forceinline__ void fused_publish(const FusedCtl& f, uint32_t C) {
+    for (uint32_t r = 1; r < C; ++r) {
+        const uint32_t a = rank_addr(&f, r);
+        st_cluster_i32(a + offsetof(FusedCtl, active), f.active);
+        st_cluster_i32(a + offsetof(FusedCtl, parity), f.parity);
+        st_cluster_i32(a + offsetof(FusedCtl, pending), f.pending);
+        st_cluster(a + offsetof(FusedCtl, mult_primal), f.mult_primal);
+        st_cluster(a + offsetof(FusedCtl, mult_dual), f.mult_dual);
+        st_cluster(a + offsetof(FusedCtl, frac), f.frac);
+    }
+}
+
+// One warp's slice of one side, staged in shared memory for the launch: the
+// cluster barriers between the halves acquire at cluster scope, after which
+// the SM's L1 holds nothing of global memory, so the slice's entries and its
+// lines' constants would otherwise come from L2 in every trial.
+template <class T>
+struct FusedLane {
+    const int32_t* idx;   // [32 * steps], the layout of the slice data
+    const T* val;
+    const T* k;           // line constants [consts][32]
+    LanePos lp;
+    int steps, len;
+    bool has, owner;
+};
+
+template <class T>
+__device__ __forceinline__ void fused_stage(const Side& side, const T* vals, int64_t data_base, int len_base,
+                                            int s, bool has, unsigned char* dst, const T* const* consts,
+                                            int nconsts, int lane, FusedLane<T>& L) {
+    L.has = has;
+    L.owner = false;
+    L.steps = 0;
+    L.len = 0;
+    if (!has) return;
+    const SliceDesc sd = side.slices[s];
+    L.lp = lane_pos(sd, lane);
+    L.owner = L.lp.valid && L.lp.g == 0;
+    L.steps = sd.steps;
+    L.len = L.lp.valid ? side.line_len[len_base + L.lp.line] : 0;
+    int32_t* idx = reinterpret_cast<int32_t*>(dst);
+    T* val = reinterpret_cast<T*>(dst + 4 * 32 * sd.steps);
+    T* k = val + 32 * sd.steps;
+    const int64_t base = data_base + static_cast<int64_t>(sd.data_off) * 32;
+    for (int q = lane; q < 32 * sd.steps; q += 32) {
+        idx[q] = side.idx[base + q];
+        val[q] = vals[base + q];
+    }
+    for (int c = 0; c < nconsts; ++c) k[c * 32 + lane] = L.owner ? consts[c][L.lp.line] : T(0);
+    __syncwarp();
+    L.idx = idx;
+    L.val = val;
+    L.k = k;
+}
+
+// line_sums over a staged slice: the same products added in the same order
+// (steps 0, 1, ... of the lane, then the lane group's butterfly), with eight
+// gathers in flight since the entries come from shared memory.
+template <int V, class T>
+__device__ __forceinline__ void staged_sums(const FusedLane<T>& L, int lane, const T* __restrict__ src,
+                                            T (&acc)[1]) {
+    constexpr int kAhead = 8;
+    for (int s0 = 0; s0 < L.steps; s0 += kAhead) {
+        T gv[kAhead], wv[kAhead];
+#pragma unroll
+        for (int u = 0; u < kAhead; ++u) {
+            const int st = s0 + u;
+            gv[u] = T(0);
+            wv[u] = T(0);
+            if (st < L.steps && (st << L.lp.glog) + L.lp.g < L.len) {
+                const int q = (st / V) * (32 * V) + lane * V + st % V;
+                wv[u] = L.val[q];
+                gv[u] = __ldcg(src + L.idx[q]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kAhead; ++u) {
+            const int st = s0 + u;
+            if (st < L.steps && (st << L.lp.glog) + L.lp.g < L.len) acc[0] += wv[u] * gv[u];
+        }
+    }
+    for (int o = (1 << L.lp.glog) >> 1; o > 0; o >>= 1) acc[0] += __shfl_xor_sync(kFull, acc[0], o);
+}
+
+// fused_primal over the warp's staged slice.
+template <class T, int V>
+__device__ __forceinline__ double fused_primal_staged(const Work<T>& w, const InstanceInfo& inf, const FusedCtl& f,
+                                                      const FusedLane<T>& L, int lane) {
+    const int p = f.parity;
+    const T mult = static_cast<T>(f.mult_primal);
+    const bool pending = f.pending != 0;
+    const T frac = static_cast<T>(f.frac);
+    const T* y = w.Y[p] + inf.row_off;
+    const T* x = w.X[p] + inf.col_off;
+    T* xt = w.X[p ^ 1] + inf.col_off;
+    T* avg = w.avg_x + inf.col_off;
+    const int j = L.lp.line;
+    T prev = T(0), aj = T(0);
+    if (L.owner) {
+        prev = __ldcg(x + j);
+        if (pending) aj = __ldcg(avg + j);
+    }
+    T sum[1] = {T(0)};
+    staged_sums<V>(L, lane, y, sum);
+    double moved = 0.0;
+    if (L.owner) {
+        const T cj = L.k[lane], loj = L.k[32 + lane], hij = L.k[64 + lane];
+        const T tj = L.k[96 + lane], itj = L.k[128 + lane];
+        const T gradient = cj + sum[0];
+        const T upd = smax(loj, smin(prev - mult * tj * gradient, hij));
+        xt[j] = upd;
+        const double d = static_cast<double>(upd - prev);
+        moved += d * d * static_cast<double>(itj);
+        if (pending) avg[j] = aj + frac * (prev - aj);
+    }
+    return moved;
+}
+
+// fused_dual over the warp's staged slice.
+template <class T, int V>
+__device__ __forceinline__ void fused_dual_staged(const Work<T>& w, const InstanceInfo& inf, const FusedCtl& f,
+                                                  const FusedLane<T>& L, int lane, double (&red)[2]) {
+    const int p = f.parity;
+    const T dm = static_cast<T>(f.mult_dual);
+    const bool pending = f.pending != 0;
+    const T frac = static_cast<T>(f.frac);
+    const T* xt = w.X[p ^ 1] + inf.col_off;
+    const T* y = w.Y[p] + inf.row_off;
+    T* yt = w.Y[p ^ 1] + inf.row_off;
+    const T* ax = w.AX[p] + inf.row_off;
+    T* axt = w.AX[p ^ 1] + inf.row_off;
+    T* avg = w.avg_y + inf.row_off;
+    const int i = L.lp.line;
+    T axi = T(0), prev = T(0), ai = T(0);
+    if (L.owner) {
+        axi = __ldcg(ax + i);
+        prev = __ldcg(y + i);
+        if (pending) ai = __ldcg(avg + i);
+    }
+    T sum[1] = {T(0)};
+    staged_sums<V>(L, lane, xt, sum);
+    if (L.owner) {
+        const T sgi = L.k[lane], isi = L.k[32 + lane], loi = L.k[64 + lane], hii = L.k[96 + lane];
+        const T next = sum[0];
+        const T dact = next - axi;
+        const T ext = next + dact;
+        const T step = smax(dm * sgi, min_dual_step<T>());
+        const T v = prev + step * ext;
+        const T upd = smax(v - step * hii, T(0)) + smin(v - step * loi, T(0));
+        yt[i] = upd;
+        axt[i] = next;
+        const double d = static_cast<double>(upd - prev);
+        red[0] += d * d * static_cast<double>(isi);
+        red[1] += d * static_cast<double>(dact);
+        if (pending) avg[i] = ai + frac * (prev - ai);
+    }
+}
+
+// One thread per CTA-map entry of rank 0 replaces the entry's slice sums
+// (`nq` values per slice) by their in-order total, stored at the entry's
+// first slice. Table word: first slice << 4 | slice count.
+__device__ __forceinline__ void fused_entry_totals(const int32_t* tab, int entries, double* part, int nq) {
+    for (int e = static_cast<int>(threadIdx.x); e < entries; e += kFusedThreads) {
+        const int first = tab[e] >> 4, cnt = tab[e] & 15;
+        if (cnt == 0) continue;
+        for (int q = 0; q < nq; ++q) {
+            double t = 0.0;
+            for (int k = 0; k < cnt; ++k) t += part[(first + k) * nq + q];
+            part[first * nq + q] = t;
+        }
+    }
+}
+
+__device__ __forceinline__ double fused_entry(const int32_t* tab, int e, const double* part, int nq, int q) {
+    return (tab[e] & 15) ? part[(tab[e] >> 4) * nq + q] : 0.0;
+}
 
 template <class T, int V>
 __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w, DeviceOptions o,
-                                                           int max_trials) {
+                                                           int max_trials, FusedShape fs) {
     // Rank 0 keeps the instance's control block in its shared memory for the
-    // whole launch (the decision's reads and writes stay on chip), publishes
-    // each trial's snapshot in `f`, and receives every group's partial sums in
-    // `part_p` / `part_d` through distributed shared memory; the other CTAs
-    // read `f` from rank 0 after each barrier. The block goes back to global
-    // memory when the launch ends.
+    // whole launch (the decision's reads and writes stay on chip), writes
+    // each trial's snapshot into every CTA's `f`, and receives every slice's
+    // warp sums in `part_p` / `part_d` through distributed shared memory. The
+    // block goes back to global memory when the launch ends.
     __shared__ DeviceOptions so;
     __shared__ FusedCtl f;
     __shared__ alignas(16) InstanceCtl sctl;
-    __shared__ double part_p[kFusedMaxEntries];
-    __shared__ double part_d[2 * kFusedMaxEntries];
+    extern __shared__ __align__(16) unsigned char fused_smem[];
+    double* const part_p = reinterpret_cast<double*>(fused_smem);
+    double* const part_d = part_p + fs.slices_p;
+    int32_t* const tab_p = reinterpret_cast<int32_t*>(part_d + 2 * fs.slices_d);
+    int32_t* const tab_d = tab_p + fs.entries_p;
+    unsigned char* const stage = fused_smem + fused_stage_offset(fs);
     const uint32_t C = cluster_size(), rank = cluster_rank();
     const int b = static_cast<int>(blockIdx.x / C);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     InstanceCtl* cp = g.ctl + b;
     const InstanceInfo inf = g.info[b];
-    // One warp per CTA-map entry: entry e goes to warp e mod (cluster warps).
+    // The instance's slices are contiguous in its CTA map (append_cta_map).
+    const int ps0 = g.at.ctas[inf.at_cta_begin].slice_begin, ps1 = g.at.ctas[inf.at_cta_end - 1].slice_end;
+    const int ds0 = g.a.ctas[inf.a_cta_begin].slice_begin, ds1 = g.a.ctas[inf.a_cta_end - 1].slice_end;
+    const int ne_p = inf.at_cta_end - inf.at_cta_begin, ne_d = inf.a_cta_end - inf.a_cta_begin;
+    // One warp per slice: slice s goes to warp s mod (cluster warps).
     const int stride = static_cast<int>(C) * kFusedWarps;
     const int slot = static_cast<int>(rank) * kFusedWarps + warp;
     constexpr bool kFp64 = sizeof(T) == 8;
+    const T* vals_p = matrix_values<T>(g.at);
+    const T* vals_d = matrix_values<T>(g.a);
     if (threadIdx.x == 0) so = o;
     if (rank == 0) {
         static_assert(sizeof(InstanceCtl) % 16 == 0, "the control block copies as 16-byte words");
         if (threadIdx.x < sizeof(InstanceCtl) / 16)
             reinterpret_cast<int4*>(&sctl)[threadIdx.x] = reinterpret_cast<const int4*>(cp)[threadIdx.x];
+        for (int e = threadIdx.x; e < ne_p; e += kFusedThreads) {
+            const CtaWork cw = g.at.ctas[inf.at_cta_begin + e];
+            tab_p[e] = ((cw.slice_begin - ps0) << 4) | (cw.slice_end - cw.slice_begin);
+        }
+        for (int e = threadIdx.x; e < ne_d; e += kFusedThreads) {
+            const CtaWork cw = g.a.ctas[inf.a_cta_begin + e];
+            tab_d[e] = ((cw.slice_begin - ds0) << 4) | (cw.slice_end - cw.slice_begin);
+        }
         __syncthreads();
         if (threadIdx.x == 0) fused_snapshot(sctl, f, kFp64);
     }
-    const uint32_t f_addr = rank0_addr(&f);
+    // Staged launches give every warp at most one slice per side.
+    const bool staged = fs.stage_bytes > 0;
+    FusedLane<T> LP{}, LD{};
+    if (staged) {
+        // The warps' shares of the stage, in warp order (lane q of every
+        // warp computes warp q's bytes).
+        const int sp = ps0 + static_cast<int>(rank) * kFusedWarps + lane;
+        const int sd = ds0 + static_cast<int>(rank) * kFusedWarps + lane;
+        int need = 0;
+        if (lane < kFusedWarps) {
+            if (sp < ps1) need += fused_slice_bytes(g.at.slices[sp].steps, kFusedPrimalConsts, sizeof(T));
+            if (sd < ds1) need += fused_slice_bytes(g.a.slices[sd].steps, kFusedDualConsts, sizeof(T));
+        }
+        int incl = need;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int t = __shfl_up_sync(kFull, incl, d);
+            if (lane >= d) incl += t;
+        }
+        const int off = __shfl_sync(kFull, incl - need, warp);
+        const int s_p = ps0 + slot, s_d = ds0 + slot;
+        const T* const cp_consts[kFusedPrimalConsts] = {w.c + inf.col_off, w.xl + inf.col_off, w.xu + inf.col_off,
+                                                        w.tau + inf.col_off, w.itau + inf.col_off};
+        const T* const cd_consts[kFusedDualConsts] = {w.sigma + inf.row_off, w.isigma + inf.row_off,
+                                                      w.rl + inf.row_off, w.ru + inf.row_off};
+        fused_stage<T>(g.at, vals_p, inf.at_data_base, inf.at_len_base, s_p, s_p < ps1, stage + off, cp_consts,
+                       kFusedPrimalConsts, lane, LP);
+        const int off_d = off + (s_p < ps1 ? fused_slice_bytes(LP.steps, kFusedPrimalConsts, sizeof(T)) : 0);
+        fused_stage<T>(g.a, vals_d, inf.a_data_base, inf.a_len_base, s_d, s_d < ds1, stage + off_d, cd_consts,
+                       kFusedDualConsts, lane, LD);
+    }
     const uint32_t pp_addr = rank0_addr(part_p);
     const uint32_t pd_addr = rank0_addr(part_d);
+    // Remote shared memory is written only once every CTA of the cluster
+    // runs: the first snapshot goes out after a barrier.
+    cluster_sync_all();
+    if (rank == 0 && threadIdx.x == 0) fused_publish(f, C);
     cluster_sync_all();
     for (int t = 0; t < max_trials; ++t) {
-        if (rank != 0 && threadIdx.x == 0) {
-            f.active = ld_cluster_i32(f_addr + offsetof(FusedCtl, active));
-            f.parity = ld_cluster_i32(f_addr + offsetof(FusedCtl, parity));
-            f.pending = ld_cluster_i32(f_addr + offsetof(FusedCtl, pending));
-            f.mult_primal = ld_cluster_f64(f_addr + offsetof(FusedCtl, mult_primal));
-            f.mult_dual = ld_cluster_f64(f_addr + offsetof(FusedCtl, mult_dual));
-            f.frac = ld_cluster_f64(f_addr + offsetof(FusedCtl, frac));
-        }
-        __syncthreads();
         if (!f.active) break;
-        // An entry's slices one after another in one warp, each reduced over
-        // its lanes and added in slice order: with at most kWarps slices per
-        // entry (choose_fused), k_primal's block sum of one slice per warp.
-        for (int e = inf.at_cta_begin + slot; e < inf.at_cta_end; e += stride) {
-            const CtaWork cw = g.at.ctas[e];
-            double total = 0.0;
-            for (int s = cw.slice_begin; s < cw.slice_end; ++s) {
-                const CtaWork one{cw.instance, s, s + 1, cw.pad};
+        // The decision's step factors of this trial, loaded while the halves
+        // run.
+        double factors[2] = {0.0, 0.0};
+        bool have_factors = false;
+        if (rank == 0 && threadIdx.x == 0) {
+            const int64_t k = sctl.phase == kPhasePolish ? sctl.polish_iteration : sctl.iteration;
+            if (so.adaptive && k >= 0 && k < so.step_pow_entries) {
+                factors[0] = so.step_pow[2 * k];
+                factors[1] = so.step_pow[2 * k + 1];
+                have_factors = true;
+            }
+        }
+        if (staged) {
+            if (LP.has) {
+                double v[1] = {fused_primal_staged<T, V>(w, inf, f, LP, lane)};
+                warp_sum<1>(v);
+                if (lane == 0) st_cluster(pp_addr + 8u * static_cast<uint32_t>(ps0 + slot - ps0), v[0]);
+            }
+        } else {
+            for (int s = ps0 + slot; s < ps1; s += stride) {
+                const CtaWork one{b, s, s + 1, 0};
                 double v[1] = {fused_primal<T, V>(g, w, one, inf, f, lane)};
                 warp_sum<1>(v);
-                total += v[0];
+                if (lane == 0) st_cluster(pp_addr + 8u * static_cast<uint32_t>(s - ps0), v[0]);
             }
-            if (lane == 0) st_cluster(pp_addr + 8u * static_cast<uint32_t>(e - inf.at_cta_begin), total);
         }
         cluster_sync_all();
-        for (int e = inf.a_cta_begin + slot; e < inf.a_cta_end; e += stride) {
-            const CtaWork cw = g.a.ctas[e];
-            double total[2] = {0.0, 0.0};
-            for (int s = cw.slice_begin; s < cw.slice_end; ++s) {
-                const CtaWork one{cw.instance, s, s + 1, cw.pad};
+        if (staged) {
+            if (LD.has) {
+                double r2[2] = {0.0, 0.0};
+                fused_dual_staged<T, V>(w, inf, f, LD, lane, r2);
+                warp_sum<2>(r2);
+                if (lane == 0) {
+                    const uint32_t q = 16u * static_cast<uint32_t>(slot);
+                    st_cluster(pd_addr + q, r2[0]);
+                    st_cluster(pd_addr + q + 8u, r2[1]);
+                }
+            }
+        } else {
+            for (int s = ds0 + slot; s < ds1; s += stride) {
+                const CtaWork one{b, s, s + 1, 0};
                 double r2[2] = {0.0, 0.0};
                 fused_dual<T, V>(g, w, one, inf, f, lane, r2);
                 warp_sum<2>(r2);
-                total[0] += r2[0];
-                total[1] += r2[1];
-            }
-            if (lane == 0) {
-                const uint32_t q = 16u * static_cast<uint32_t>(e - inf.a_cta_begin);
-                st_cluster(pd_addr + q, total[0]);
-                st_cluster(pd_addr + q + 8u, total[1]);
+                if (lane == 0) {
+                    const uint32_t q = 16u * static_cast<uint32_t>(s - ds0);
+                    st_cluster(pd_addr + q, r2[0]);
+                    st_cluster(pd_addr + q + 8u, r2[1]);
+                }
             }
         }
         cluster_sync_all();
-        if (rank == 0 && threadIdx.x < 32) {
-            // k_dual's fixed-order sums over the same partials, from shared memory.
-            double sums[3];
-            warp_range_sums3<false>(part_p, 0, inf.at_cta_end - inf.at_cta_begin, 1, 0,
-                                    part_d, 0, inf.a_cta_end - inf.a_cta_begin, 2, 0,
-                                    part_d, 0, inf.a_cta_end - inf.a_cta_begin, 2, 1, sums);
-            if (threadIdx.x == 0) {
-                trial_control(sctl, so, sums[0], sums[1], sums[2], inf.n);
-                fused_snapshot(sctl, f, kFp64);
+        if (rank == 0) {
+            fused_entry_totals(tab_p, ne_p, part_p, 1);
+            fused_entry_totals(tab_d, ne_d, part_d, 2);
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                // k_dual's fixed-order sums over the entries' totals
+                // (warp_range_sums3: entries lane, lane + 32, ... in order,
+                // then the butterfly).
+                double sums[3] = {0.0, 0.0, 0.0};
+                for (int e = lane; e < ne_p; e += 32) sums[0] += fused_entry(tab_p, e, part_p, 1, 0);
+                for (int e = lane; e < ne_d; e += 32) {
+                    sums[1] += fused_entry(tab_d, e, part_d, 2, 0);
+                    sums[2] += fused_entry(tab_d, e, part_d, 2, 1);
+                }
+                warp_sum<3>(sums);
+                if (threadIdx.x == 0) {
+                    trial_control(sctl, so, sums[0], sums[1], sums[2], inf.n, have_factors ? factors : nullptr);
+                    fused_snapshot(sctl, f, kFp64);
+                    fused_publish(f, C);
+                }
             }
         }
         cluster_sync_all();
     }
-    // Every CTA left the loop at the same trial; the barrier keeps rank 0's
-    // shared memory alive until the others have read `f` from it.
+    // Every CTA left the loop at the same trial (the same snapshot after the
+    // same barrier); the barrier keeps every CTA's shared memory alive until
+    // the last remote store into it has landed.
     cluster_sync_all();
     if (rank == 0) {
         if (threadIdx.x < sizeof(InstanceCtl) / 16)
@@ -1871,10 +2124,15 @@ void launch_primal(const Global& g, const Work<T>& w, const DeviceOptions&, int 
 namespace {
 template <class T, int V>
 cudaError_t fused_v(const Global& g, const Work<T>& w, const DeviceOptions& o, int count, int cluster,
-                    int max_trials, cudaStream_t s) {
+                    int max_trials, const FusedShape& shape, cudaStream_t s) {
+    const size_t smem = fused_smem_bytes(shape);
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_fused<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(static_cast<unsigned>(count * cluster));
     cfg.blockDim = dim3(kFusedThreads);
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1885,14 +2143,20 @@ cudaError_t fused_v(const Global& g, const Work<T>& w, const DeviceOptions& o, i
     cfg.numAttrs = 1;
     // Clusters of 16 CTAs are beyond the portable size of 8.
     cudaFuncSetAttribute(k_fused<T, V>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    return cudaLaunchKernelEx(&cfg, k_fused<T, V>, g, w, o, max_trials);
+    return cudaLaunchKernelEx(&cfg, k_fused<T, V>, g, w, o, max_trials, shape);
 }
 
 template <class T, int V>
-int fused_clusters_v(int cluster) {
+int fused_clusters_v(int cluster, size_t smem) {
+    if (cudaFuncSetAttribute(k_fused<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(static_cast<unsigned>(cluster));
     cfg.blockDim = dim3(kFusedThreads);
+    cfg.dynamicSmemBytes = smem;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = static_cast<unsigned>(cluster);
@@ -1916,21 +2180,22 @@ int fused_clusters_v(int cluster) {
 
 template <class T>
 cudaError_t launch_fused(const Global& g, const Work<T>& w, const DeviceOptions& o, int vw, int count,
-                         int cluster, int max_trials, cudaStream_t s) {
+                         int cluster, int max_trials, const FusedShape& shape, cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
     switch (vw) {
-        case 4: return fused_v<T, 4>(g, w, o, count, cluster, max_trials, s);
-        case 2: return fused_v<T, 2>(g, w, o, count, cluster, max_trials, s);
-        default: return fused_v<T, 1>(g, w, o, count, cluster, max_trials, s);
+        case 4: return fused_v<T, 4>(g, w, o, count, cluster, max_trials, shape, s);
+        case 2: return fused_v<T, 2>(g, w, o, count, cluster, max_trials, shape, s);
+        default: return fused_v<T, 1>(g, w, o, count, cluster, max_trials, shape, s);
     }
 }
 
 template <class T>
-int fused_max_clusters(int vw, int cluster) {
+int fused_max_clusters(int vw, int cluster, const FusedShape& shape) {
+    const size_t smem = fused_smem_bytes(shape);
     switch (vw) {
-        case 4: return fused_clusters_v<T, 4>(cluster);
-        case 2: return fused_clusters_v<T, 2>(cluster);
-        default: return fused_clusters_v<T, 1>(cluster);
+        case 4: return fused_clusters_v<T, 4>(cluster, smem);
+        case 2: return fused_clusters_v<T, 2>(cluster, smem);
+        default: return fused_clusters_v<T, 1>(cluster, smem);
     }
 }
 
@@ -2132,8 +2397,8 @@ void launch_slot_done(const Global& g, int32_t count, int32_t* done, cudaStream_
 #define PDLPGPU_INSTANTIATE(T)                                                                      \
     template void launch_primal<T>(const Global&, const Work<T>&, const DeviceOptions&, int, cudaStream_t); \
     template cudaError_t launch_fused<T>(const Global&, const Work<T>&, const DeviceOptions&, int, int, int, \
-                                         int, cudaStream_t);                                         \
-    template int fused_max_clusters<T>(int, int);                                                    \
+                                         int, const FusedShape&, cudaStream_t);                      \
+    template int fused_max_clusters<T>(int, int, const FusedShape&);                                 \
     template void launch_dual<T>(const Global&, const Work<T>&, const DeviceOptions&, int, cudaStream_t);   \
     template void launch_check_prep<T>(const Global&, const Work<T>&, const DeviceOptions&, cudaStream_t);  \
     template void launch_check_apply<T>(const Global&, const Work<T>&, const DeviceOptions&, cudaStream_t); \

@@ -107,20 +107,44 @@ void launch_primal(const Global& g, const Work<T>& w, const DeviceOptions& o, in
 template <class T>
 void launch_dual(const Global& g, const Work<T>& w, const DeviceOptions& o, int vw,
                  cudaStream_t s);
+// The shape of a fused launch's shared memory, over its instances.
+struct FusedShape {
+    int32_t slices_p, slices_d;     // most slices of an instance per side
+    int32_t entries_p, entries_d;   // most CTA-map entries of an instance per side
+    int32_t stage_bytes;            // most bytes of a CTA's staged slices (0: nothing staged)
+};
+// Dynamic shared memory of a fused CTA: one warp sum per primal slice, two
+// per dual slice, one word per CTA-map entry, then the staged slices.
+__host__ __device__ inline size_t fused_stage_offset(const FusedShape& f) {
+    const size_t b = sizeof(double) * (static_cast<size_t>(f.slices_p) + 2 * static_cast<size_t>(f.slices_d)) +
+                     sizeof(int32_t) * (static_cast<size_t>(f.entries_p) + static_cast<size_t>(f.entries_d));
+    return (b + 15) & ~static_cast<size_t>(15);
+}
+__host__ __device__ inline size_t fused_smem_bytes(const FusedShape& f) {
+    return fused_stage_offset(f) + static_cast<size_t>(f.stage_bytes);
+}
+// A staged slice in shared memory: the index and value of each of its 32 x
+// `steps` entries, then `consts` line constants per lane (element size
+// `elem`).
+constexpr int kFusedPrimalConsts = 5;   // objective, lower, upper, tau, 1/tau
+constexpr int kFusedDualConsts = 4;     // sigma, 1/sigma, lower, upper
+__host__ __device__ constexpr int fused_slice_bytes(int steps, int consts, int elem) {
+    return 32 * steps * (4 + elem) + 32 * consts * elem;
+}
 // The trials of a check interval of `count` small instances in one launch:
 // one cluster of `cluster` CTAs (512 threads each) per instance, at most
 // `max_trials` trials each, stopping at a check or the end (kernels.cu,
 // k_fused). Same results as launch_primal + launch_dual per trial.
 template <class T>
 cudaError_t launch_fused(const Global& g, const Work<T>& w, const DeviceOptions& o, int vw, int count,
-                         int cluster, int max_trials, cudaStream_t s);
+                         int cluster, int max_trials, const FusedShape& shape, cudaStream_t s);
 // Clusters of that shape resident at once (0: the launch is not possible).
 template <class T>
-int fused_max_clusters(int vw, int cluster);
+int fused_max_clusters(int vw, int cluster, const FusedShape& shape);
 constexpr int kFusedCtaThreads = 512;
-// Entries per instance side the fused kernel's partial-sum arrays hold (four
-// rounds of the largest cluster's warps).
-constexpr int kFusedMaxEntriesHost = 1024;
+// Largest dynamic shared memory the engine gives a fused CTA (its static
+// shared memory, the control block and the options, fit beside it).
+constexpr size_t kFusedMaxSmemHost = 200 * 1024;
 template <class T>
 void launch_check_prep(const Global& g, const Work<T>& w, const DeviceOptions& o, cudaStream_t s);
 void launch_check_spmv(const Global& g, const DeviceOptions& o, int vw, cudaStream_t s);

@@ -5,7 +5,8 @@ CTA), so a solve must give the same statuses, counters and points bit for bit
 with either; `two_kernel_trials=1` forces the two-kernel path. Cases: the
 1000 x 2000 planted LP (FP64 and mixed through its FP64 stage), the
 reference's KATs (infeasible, unbounded, polishing after an iteration limit),
-a batch of different LPs, and the per-iteration time of both paths.
+a 10000 x 20000 LP too large to stage its slices in shared memory, a batch of
+different LPs, and the per-iteration time of both paths.
 """
 import time
 
@@ -45,6 +46,9 @@ CASES = [
     ("limit_then_polish", lambda: cases.random_feasible(300, 420, 21), "fp64",
      cases.convergence_options(iteration_limit=150, use_feasibility_polishing=True,
                                polishing_iterations=300)),
+    # 625 column slices: more than a 16-CTA cluster has warps, so the slices
+    # are read from global memory in every trial instead of being staged.
+    ("planted_10k_unstaged", lambda: g.planted_lp(10000, 20000, seed=4).lp, "mixed", _opts(1e-5)),
 ]
 
 
