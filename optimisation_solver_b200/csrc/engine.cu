@@ -888,7 +888,8 @@ int Engine::timed_position(int k, int slots) const {
 // instances whose slices' warp sums fit a CTA's shared memory, when the
 // device can hold such a cluster. When the cluster has a warp for every
 // slice and the warps' slices fit beside the sums, the slices are staged in
-// shared memory for the launch.
+// shared memory for the launch, and when x and y fit beside them too, every
+// CTA keeps copies of them and no trial touches global memory.
 void Engine::choose_fused() {
     fused_cluster_ = 0;
     fused_shape_ = FusedShape{};
@@ -925,34 +926,44 @@ void Engine::choose_fused() {
     if (resident(cluster, sh) <= 0) return;
     if (cluster * warps_per_cta >= std::max(sh.slices_p, sh.slices_d)) {
         // Staging: CTA rank r's warp q takes slice r * 16 + q of each side;
-        // its bytes at the FP64 element size (the larger of the two stages).
-        int64_t stage = 0;
-        for (int b = 0; b < count_; ++b) {
-            const InstanceInfo& inf = info_[static_cast<size_t>(b)];
-            const MatrixLayout& L = layouts_[spec_.shared_matrix ? 0 : b];
-            const int ps0 = first(at_ctas_, inf.at_cta_begin) - inf.at_slice_base;
-            const int ps1 = last(at_ctas_, inf.at_cta_end) - inf.at_slice_base;
-            const int ds0 = first(a_ctas_, inf.a_cta_begin) - inf.a_slice_base;
-            const int ds1 = last(a_ctas_, inf.a_cta_end) - inf.a_slice_base;
-            for (int r = 0; r < cluster; ++r) {
-                int64_t cta = 0;
-                for (int q = 0; q < warps_per_cta; ++q) {
-                    const int k = r * warps_per_cta + q;
-                    if (ps0 + k < ps1)
-                        cta += fused_slice_bytes(L.at.slices[static_cast<size_t>(ps0 + k)].steps, kFusedPrimalConsts,
-                                                 static_cast<int>(sizeof(double)));
-                    if (ds0 + k < ds1)
-                        cta += fused_slice_bytes(L.a.slices[static_cast<size_t>(ds0 + k)].steps, kFusedDualConsts,
-                                                 static_cast<int>(sizeof(double)));
+        // its bytes at the FP64 element size (the larger of the two stages),
+        // with or without the lines' own iterates.
+        auto stage_bytes = [&](int own_p, int own_d) {
+            int64_t stage = 0;
+            for (int b = 0; b < count_; ++b) {
+                const InstanceInfo& inf = info_[static_cast<size_t>(b)];
+                const MatrixLayout& L = layouts_[spec_.shared_matrix ? 0 : b];
+                const int ps0 = first(at_ctas_, inf.at_cta_begin) - inf.at_slice_base;
+                const int ps1 = last(at_ctas_, inf.at_cta_end) - inf.at_slice_base;
+                const int ds0 = first(a_ctas_, inf.a_cta_begin) - inf.a_slice_base;
+                const int ds1 = last(a_ctas_, inf.a_cta_end) - inf.a_slice_base;
+                for (int r = 0; r < cluster; ++r) {
+                    int64_t cta = 0;
+                    for (int q = 0; q < warps_per_cta; ++q) {
+                        const int k = r * warps_per_cta + q;
+                        if (ps0 + k < ps1)
+                            cta += fused_slice_bytes(L.at.slices[static_cast<size_t>(ps0 + k)].steps,
+                                                     kFusedPrimalConsts + own_p, static_cast<int>(sizeof(double)));
+                        if (ds0 + k < ds1)
+                            cta += fused_slice_bytes(L.a.slices[static_cast<size_t>(ds0 + k)].steps,
+                                                     kFusedDualConsts + own_d, static_cast<int>(sizeof(double)));
+                    }
+                    stage = std::max(stage, cta);
                 }
-                stage = std::max(stage, cta);
             }
-        }
+            // Never zero when staged (the kernel tells the modes apart by it).
+            return static_cast<int32_t>(std::max<int64_t>(16, std::min<int64_t>(stage, INT32_MAX)));
+        };
+        int32_t lines = 0;
+        for (int b = 0; b < count_; ++b)
+            lines = std::max(lines, info_[static_cast<size_t>(b)].m + info_[static_cast<size_t>(b)].n);
+        FusedShape copies = sh;
+        copies.stage_bytes = stage_bytes(kFusedPrimalOwn, kFusedDualOwn);
+        copies.lines = lines;
         FusedShape staged = sh;
-        staged.stage_bytes = static_cast<int32_t>(std::min<int64_t>(stage, INT32_MAX));
-        // Never zero when staged (the kernel tells the two modes apart by it).
-        staged.stage_bytes = std::max(staged.stage_bytes, 16);
-        if (fused_smem_bytes(staged) <= kFusedMaxSmemHost && resident(cluster, staged) > 0) sh = staged;
+        staged.stage_bytes = stage_bytes(0, 0);
+        if (fused_smem_bytes(copies) <= kFusedMaxSmemHost && resident(cluster, copies) > 0) sh = copies;
+        else if (fused_smem_bytes(staged) <= kFusedMaxSmemHost && resident(cluster, staged) > 0) sh = staged;
     }
     fused_cluster_ = cluster;
     fused_shape_ = sh;

@@ -682,15 +682,19 @@ struct FusedLane {
     const int32_t* idx;   // [32 * steps], the layout of the slice data
     const T* val;
     const T* k;           // line constants [consts][32]
+    T* v;                 // the lines' own iterates [vecs][32] (launches with copies)
     LanePos lp;
     int steps, len;
     bool has, owner;
 };
 
+// Carves the warp's region of one side: the slice's entries, its lines'
+// constants and, with copies, the lines' own iterates (`nvecs` vectors).
 template <class T>
 __device__ __forceinline__ void fused_stage(const Side& side, const T* vals, int64_t data_base, int len_base,
                                             int s, bool has, unsigned char* dst, const T* const* consts,
-                                            int nconsts, int lane, FusedLane<T>& L) {
+                                            int nconsts, const T* const* vecs, int nvecs, int lane,
+                                            FusedLane<T>& L) {
     L.has = has;
     L.owner = false;
     L.steps = 0;
@@ -710,18 +714,21 @@ __device__ __forceinline__ void fused_stage(const Side& side, const T* vals, int
         val[q] = vals[base + q];
     }
     for (int c = 0; c < nconsts; ++c) k[c * 32 + lane] = L.owner ? consts[c][L.lp.line] : T(0);
+    T* v = k + 32 * nconsts;
+    for (int c = 0; c < nvecs; ++c) v[c * 32 + lane] = L.owner ? vecs[c][L.lp.line] : T(0);
     __syncwarp();
     L.idx = idx;
     L.val = val;
     L.k = k;
+    L.v = v;
 }
 
 // line_sums over a staged slice: the same products added in the same order
 // (steps 0, 1, ... of the lane, then the lane group's butterfly), with eight
-// gathers in flight since the entries come from shared memory.
-template <int V, class T>
-__device__ __forceinline__ void staged_sums(const FusedLane<T>& L, int lane, const T* __restrict__ src,
-                                            T (&acc)[1]) {
+// gathers in flight since the entries come from shared memory; `get(i)`
+// gathers element i of the other side's vector.
+template <int V, class T, class Get>
+__device__ __forceinline__ void staged_sums(const FusedLane<T>& L, int lane, Get get, T (&acc)[1]) {
     constexpr int kAhead = 8;
     for (int s0 = 0; s0 < L.steps; s0 += kAhead) {
         T gv[kAhead], wv[kAhead];
@@ -733,7 +740,7 @@ __device__ __forceinline__ void staged_sums(const FusedLane<T>& L, int lane, con
             if (st < L.steps && (st << L.lp.glog) + L.lp.g < L.len) {
                 const int q = (st / V) * (32 * V) + lane * V + st % V;
                 wv[u] = L.val[q];
-                gv[u] = __ldcg(src + L.idx[q]);
+                gv[u] = get(L.idx[q]);
             }
         }
 #pragma unroll
@@ -764,7 +771,7 @@ __device__ __forceinline__ double fused_primal_staged(const Work<T>& w, const In
         if (pending) aj = __ldcg(avg + j);
     }
     T sum[1] = {T(0)};
-    staged_sums<V>(L, lane, y, sum);
+    staged_sums<V>(L, lane, [&](int i) { return __ldcg(y + i); }, sum);
     double moved = 0.0;
     if (L.owner) {
         const T cj = L.k[lane], loj = L.k[32 + lane], hij = L.k[64 + lane];
@@ -801,7 +808,7 @@ __device__ __forceinline__ void fused_dual_staged(const Work<T>& w, const Instan
         if (pending) ai = __ldcg(avg + i);
     }
     T sum[1] = {T(0)};
-    staged_sums<V>(L, lane, xt, sum);
+    staged_sums<V>(L, lane, [&](int j) { return __ldcg(xt + j); }, sum);
     if (L.owner) {
         const T sgi = L.k[lane], isi = L.k[32 + lane], loi = L.k[64 + lane], hii = L.k[96 + lane];
         const T next = sum[0];
@@ -816,6 +823,98 @@ __device__ __forceinline__ void fused_dual_staged(const Work<T>& w, const Instan
         red[0] += d * d * static_cast<double>(isi);
         red[1] += d * static_cast<double>(dact);
         if (pending) avg[i] = ai + frac * (prev - ai);
+    }
+}
+
+// Launches with copies: every CTA holds the instance's whole x and y (both
+// parities) in its shared memory, so the gathers are local; the owner lane of
+// a line writes its new value into every CTA's copy (the lanes of a slice own
+// consecutive lines, so each remote store is one contiguous run), and keeps
+// the line's average (and Ax) in its own region. No trial touches global
+// memory.
+template <class T>
+struct FusedCopies {
+    T* x[2];   // [n] each, this CTA's copy
+    T* y[2];   // [m] each
+};
+
+// The value v of element `e` of a copied vector, stored into all C copies.
+template <class T>
+__device__ __forceinline__ void store_copies(const T* elem, T v, uint32_t C);
+template <>
+__device__ __forceinline__ void store_copies<double>(const double* elem, double v, uint32_t C) {
+    for (uint32_t r = 0; r < C; ++r) st_cluster(rank_addr(elem, r), v);
+}
+template <>
+__device__ __forceinline__ void store_copies<float>(const float* elem, float v, uint32_t C) {
+    for (uint32_t r = 0; r < C; ++r)
+        asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(rank_addr(elem, r)), "f"(v) : "memory");
+}
+
+// fused_primal with copies; own region: the line's average.
+template <class T, int V>
+__device__ __forceinline__ double fused_primal_copies(const FusedCtl& f, const FusedLane<T>& L,
+                                                      const FusedCopies<T>& cc, uint32_t C, int lane) {
+    const int p = f.parity;
+    const T mult = static_cast<T>(f.mult_primal);
+    const bool pending = f.pending != 0;
+    const T frac = static_cast<T>(f.frac);
+    const T* y = cc.y[p];
+    const int j = L.lp.line;
+    T prev = T(0), aj = T(0);
+    if (L.owner) {
+        prev = cc.x[p][j];
+        if (pending) aj = L.v[lane];
+    }
+    T sum[1] = {T(0)};
+    staged_sums<V>(L, lane, [&](int i) { return y[i]; }, sum);
+    double moved = 0.0;
+    if (L.owner) {
+        const T cj = L.k[lane], loj = L.k[32 + lane], hij = L.k[64 + lane];
+        const T tj = L.k[96 + lane], itj = L.k[128 + lane];
+        const T gradient = cj + sum[0];
+        const T upd = smax(loj, smin(prev - mult * tj * gradient, hij));
+        store_copies<T>(cc.x[p ^ 1] + j, upd, C);
+        const double d = static_cast<double>(upd - prev);
+        moved += d * d * static_cast<double>(itj);
+        if (pending) L.v[lane] = aj + frac * (prev - aj);
+    }
+    return moved;
+}
+
+// fused_dual with copies; own region: Ax of both parities, the average.
+template <class T, int V>
+__device__ __forceinline__ void fused_dual_copies(const FusedCtl& f, const FusedLane<T>& L,
+                                                  const FusedCopies<T>& cc, uint32_t C, int lane,
+                                                  double (&red)[2]) {
+    const int p = f.parity;
+    const T dm = static_cast<T>(f.mult_dual);
+    const bool pending = f.pending != 0;
+    const T frac = static_cast<T>(f.frac);
+    const T* xt = cc.x[p ^ 1];
+    const int i = L.lp.line;
+    T axi = T(0), prev = T(0), ai = T(0);
+    if (L.owner) {
+        axi = L.v[p * 32 + lane];
+        prev = cc.y[p][i];
+        if (pending) ai = L.v[64 + lane];
+    }
+    T sum[1] = {T(0)};
+    staged_sums<V>(L, lane, [&](int jj) { return xt[jj]; }, sum);
+    if (L.owner) {
+        const T sgi = L.k[lane], isi = L.k[32 + lane], loi = L.k[64 + lane], hii = L.k[96 + lane];
+        const T next = sum[0];
+        const T dact = next - axi;
+        const T ext = next + dact;
+        const T step = smax(dm * sgi, min_dual_step<T>());
+        const T v = prev + step * ext;
+        const T upd = smax(v - step * hii, T(0)) + smin(v - step * loi, T(0));
+        store_copies<T>(cc.y[p ^ 1] + i, upd, C);
+        L.v[(p ^ 1) * 32 + lane] = next;
+        const double d = static_cast<double>(upd - prev);
+        red[0] += d * d * static_cast<double>(isi);
+        red[1] += d * static_cast<double>(dact);
+        if (pending) L.v[64 + lane] = ai + frac * (prev - ai);
     }
 }
 
@@ -855,6 +954,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
     int32_t* const tab_p = reinterpret_cast<int32_t*>(part_d + 2 * fs.slices_d);
     int32_t* const tab_d = tab_p + fs.entries_p;
     unsigned char* const stage = fused_smem + fused_stage_offset(fs);
+    T* const copies = reinterpret_cast<T*>(fused_smem + fused_copies_offset(fs));
     const uint32_t C = cluster_size(), rank = cluster_rank();
     const int b = static_cast<int>(blockIdx.x / C);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -886,9 +986,34 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
         __syncthreads();
         if (threadIdx.x == 0) fused_snapshot(sctl, f, kFp64);
     }
-    // Staged launches give every warp at most one slice per side.
+    // Staged launches give every warp at most one slice per side; with
+    // copies, the x and y of both parities are in every CTA.
     const bool staged = fs.stage_bytes > 0;
+    const bool with_copies = staged && fs.lines > 0;
     FusedLane<T> LP{}, LD{};
+    FusedCopies<T> cc{};
+    T* const xg[2] = {w.X[0] + inf.col_off, w.X[1] + inf.col_off};
+    T* const yg[2] = {w.Y[0] + inf.row_off, w.Y[1] + inf.row_off};
+    // The lines' own iterates with copies: primal the average; dual Ax of
+    // both parities, the average.
+    const T* const own_p[1] = {w.avg_x + inf.col_off};
+    const T* const own_d[3] = {w.AX[0] + inf.row_off, w.AX[1] + inf.row_off, w.avg_y + inf.row_off};
+    const int words_p = kFusedPrimalConsts + (with_copies ? kFusedPrimalOwn : 0);
+    const int words_d = kFusedDualConsts + (with_copies ? kFusedDualOwn : 0);
+    if (with_copies) {
+        cc.x[0] = copies;
+        cc.x[1] = copies + inf.n;
+        cc.y[0] = copies + 2 * inf.n;
+        cc.y[1] = copies + 2 * inf.n + inf.m;
+        for (int q = threadIdx.x; q < inf.n; q += kFusedThreads) {
+            cc.x[0][q] = xg[0][q];
+            cc.x[1][q] = xg[1][q];
+        }
+        for (int q = threadIdx.x; q < inf.m; q += kFusedThreads) {
+            cc.y[0][q] = yg[0][q];
+            cc.y[1][q] = yg[1][q];
+        }
+    }
     if (staged) {
         // The warps' shares of the stage, in warp order (lane q of every
         // warp computes warp q's bytes).
@@ -896,8 +1021,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
         const int sd = ds0 + static_cast<int>(rank) * kFusedWarps + lane;
         int need = 0;
         if (lane < kFusedWarps) {
-            if (sp < ps1) need += fused_slice_bytes(g.at.slices[sp].steps, kFusedPrimalConsts, sizeof(T));
-            if (sd < ds1) need += fused_slice_bytes(g.a.slices[sd].steps, kFusedDualConsts, sizeof(T));
+            if (sp < ps1) need += fused_slice_bytes(g.at.slices[sp].steps, words_p, sizeof(T));
+            if (sd < ds1) need += fused_slice_bytes(g.a.slices[sd].steps, words_d, sizeof(T));
         }
         int incl = need;
         for (int d = 1; d < 32; d <<= 1) {
@@ -911,10 +1036,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
         const T* const cd_consts[kFusedDualConsts] = {w.sigma + inf.row_off, w.isigma + inf.row_off,
                                                       w.rl + inf.row_off, w.ru + inf.row_off};
         fused_stage<T>(g.at, vals_p, inf.at_data_base, inf.at_len_base, s_p, s_p < ps1, stage + off, cp_consts,
-                       kFusedPrimalConsts, lane, LP);
-        const int off_d = off + (s_p < ps1 ? fused_slice_bytes(LP.steps, kFusedPrimalConsts, sizeof(T)) : 0);
+                       kFusedPrimalConsts, own_p, with_copies ? kFusedPrimalOwn : 0, lane, LP);
+        const int off_d = off + (s_p < ps1 ? fused_slice_bytes(LP.steps, words_p, sizeof(T)) : 0);
         fused_stage<T>(g.a, vals_d, inf.a_data_base, inf.a_len_base, s_d, s_d < ds1, stage + off_d, cd_consts,
-                       kFusedDualConsts, lane, LD);
+                       kFusedDualConsts, own_d, with_copies ? kFusedDualOwn : 0, lane, LD);
     }
     const uint32_t pp_addr = rank0_addr(part_p);
     const uint32_t pd_addr = rank0_addr(part_d);
@@ -937,7 +1062,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
                 have_factors = true;
             }
         }
-        if (staged) {
+        if (with_copies) {
+            if (LP.has) {
+                double v[1] = {fused_primal_copies<T, V>(f, LP, cc, C, lane)};
+                warp_sum<1>(v);
+                if (lane == 0) st_cluster(pp_addr + 8u * static_cast<uint32_t>(slot), v[0]);
+            }
+        } else if (staged) {
             if (LP.has) {
                 double v[1] = {fused_primal_staged<T, V>(w, inf, f, LP, lane)};
                 warp_sum<1>(v);
@@ -952,7 +1083,18 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
             }
         }
         cluster_sync_all();
-        if (staged) {
+        if (with_copies) {
+            if (LD.has) {
+                double r2[2] = {0.0, 0.0};
+                fused_dual_copies<T, V>(f, LD, cc, C, lane, r2);
+                warp_sum<2>(r2);
+                if (lane == 0) {
+                    const uint32_t q = 16u * static_cast<uint32_t>(slot);
+                    st_cluster(pd_addr + q, r2[0]);
+                    st_cluster(pd_addr + q + 8u, r2[1]);
+                }
+            }
+        } else if (staged) {
             if (LD.has) {
                 double r2[2] = {0.0, 0.0};
                 fused_dual_staged<T, V>(w, inf, f, LD, lane, r2);
@@ -1005,6 +1147,27 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
     // same barrier); the barrier keeps every CTA's shared memory alive until
     // the last remote store into it has landed.
     cluster_sync_all();
+    if (with_copies) {
+        // Every copy is the same: rank 0 writes x and y back, the owner lanes
+        // their lines' own iterates.
+        if (rank == 0) {
+            for (int q = threadIdx.x; q < inf.n; q += kFusedThreads) {
+                xg[0][q] = cc.x[0][q];
+                xg[1][q] = cc.x[1][q];
+            }
+            for (int q = threadIdx.x; q < inf.m; q += kFusedThreads) {
+                yg[0][q] = cc.y[0][q];
+                yg[1][q] = cc.y[1][q];
+            }
+        }
+        if (LP.has && LP.owner) w.avg_x[inf.col_off + LP.lp.line] = LP.v[lane];
+        if (LD.has && LD.owner) {
+            const int i = inf.row_off + LD.lp.line;
+            w.AX[0][i] = LD.v[lane];
+            w.AX[1][i] = LD.v[32 + lane];
+            w.avg_y[i] = LD.v[64 + lane];
+        }
+    }
     if (rank == 0) {
         if (threadIdx.x < sizeof(InstanceCtl) / 16)
             reinterpret_cast<int4*>(cp)[threadIdx.x] = reinterpret_cast<const int4*>(&sctl)[threadIdx.x];

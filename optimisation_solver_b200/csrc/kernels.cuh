@@ -112,13 +112,18 @@ struct FusedShape {
     int32_t slices_p, slices_d;     // most slices of an instance per side
     int32_t entries_p, entries_d;   // most CTA-map entries of an instance per side
     int32_t stage_bytes;            // most bytes of a CTA's staged slices (0: nothing staged)
+    int32_t lines;                  // staged with copies: most rows + columns of an instance (else 0)
 };
 // Dynamic shared memory of a fused CTA: one warp sum per primal slice, two
-// per dual slice, one word per CTA-map entry, then the staged slices.
-__host__ __device__ inline size_t fused_stage_offset(const FusedShape& f) {
+// per dual slice, one word per CTA-map entry; then, with copies, x and y of
+// both parities (sized for FP64); then the staged slices.
+__host__ __device__ inline size_t fused_copies_offset(const FusedShape& f) {
     const size_t b = sizeof(double) * (static_cast<size_t>(f.slices_p) + 2 * static_cast<size_t>(f.slices_d)) +
                      sizeof(int32_t) * (static_cast<size_t>(f.entries_p) + static_cast<size_t>(f.entries_d));
     return (b + 15) & ~static_cast<size_t>(15);
+}
+__host__ __device__ inline size_t fused_stage_offset(const FusedShape& f) {
+    return fused_copies_offset(f) + 2 * sizeof(double) * static_cast<size_t>(f.lines);
 }
 __host__ __device__ inline size_t fused_smem_bytes(const FusedShape& f) {
     return fused_stage_offset(f) + static_cast<size_t>(f.stage_bytes);
@@ -128,6 +133,9 @@ __host__ __device__ inline size_t fused_smem_bytes(const FusedShape& f) {
 // `elem`).
 constexpr int kFusedPrimalConsts = 5;   // objective, lower, upper, tau, 1/tau
 constexpr int kFusedDualConsts = 4;     // sigma, 1/sigma, lower, upper
+// With copies, the lines' own iterates follow the constants.
+constexpr int kFusedPrimalOwn = 1;      // the average
+constexpr int kFusedDualOwn = 3;        // Ax of both parities, the average
 __host__ __device__ constexpr int fused_slice_bytes(int steps, int consts, int elem) {
     return 32 * steps * (4 + elem) + 32 * consts * elem;
 }
@@ -144,7 +152,7 @@ int fused_max_clusters(int vw, int cluster, const FusedShape& shape);
 constexpr int kFusedCtaThreads = 512;
 // Largest dynamic shared memory the engine gives a fused CTA (its static
 // shared memory, the control block and the options, fit beside it).
-constexpr size_t kFusedMaxSmemHost = 200 * 1024;
+constexpr size_t kFusedMaxSmemHost = 224 * 1024;
 template <class T>
 void launch_check_prep(const Global& g, const Work<T>& w, const DeviceOptions& o, cudaStream_t s);
 void launch_check_spmv(const Global& g, const DeviceOptions& o, int vw, cudaStream_t s);
