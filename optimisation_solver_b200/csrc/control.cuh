@@ -185,6 +185,13 @@ __device__ inline void loop_top_main(InstanceCtl& c, const DeviceOptions& o, int
     c.stage = kStageTrial;
 }
 
+// k % q (q > 0, validated at setup) in 32-bit arithmetic while k fits: the
+// same value at a fraction of a 64-bit remainder's cost.
+__device__ __forceinline__ int64_t count_mod(int64_t k, int32_t q) {
+    if (k >= 0 && k <= 0x7fffffff) return static_cast<int32_t>(k) % q;
+    return k % q;
+}
+
 __device__ inline void average_add(InstanceCtl& c, double weight) {   // iterate_average.cpp:40-82
     if (!(weight > 0.0)) return;
     const double total = c.avg_weight + weight;
@@ -250,7 +257,7 @@ inline __device__ __noinline__ void trial_control(InstanceCtl& c, const DeviceOp
         ++c.iteration;
         ++c.since_restart;
         if (o.averaging) average_add(c, c.eta);
-        if (c.iteration % o.check_frequency == 0) {
+        if (count_mod(c.iteration, o.check_frequency) == 0) {
             c.stage = kStageCheck;
             c.check_kind = kCheckMain;
         } else {
@@ -261,7 +268,7 @@ inline __device__ __noinline__ void trial_control(InstanceCtl& c, const DeviceOp
         ++c.polish_done_iterations;
         if (o.averaging) average_add(c, c.trial_eta);
         const bool last = c.polish_done_iterations == o.polishing_iterations;
-        if (c.polish_done_iterations % o.check_frequency == 0 || last) {
+        if (count_mod(c.polish_done_iterations, o.check_frequency) == 0 || last) {
             c.stage = kStageCheck;
             c.check_kind = kCheckPolish;
         }

@@ -897,13 +897,17 @@ void Engine::choose_fused() {
     // The fused kernel adds an entry's slice sums in slice order; that
     // equals the two-kernel path's block sum (one slice per warp, warps in
     // order) only while no entry has more slices than a CTA has warps.
+    bool multi = false;
     for (const auto* side : {&a_ctas_, &at_ctas_})
-        for (const CtaWork& cw : *side)
+        for (const CtaWork& cw : *side) {
             if (cw.slice_end - cw.slice_begin > kThreads / 32) return;
+            multi = multi || cw.slice_end - cw.slice_begin != 1;
+        }
     // An instance's slices are contiguous in its CTA map.
     auto first = [](const std::vector<CtaWork>& side, int e0) { return side[static_cast<size_t>(e0)].slice_begin; };
     auto last = [](const std::vector<CtaWork>& side, int e1) { return side[static_cast<size_t>(e1 - 1)].slice_end; };
     FusedShape sh{};
+    sh.multi = multi ? 1 : 0;
     for (int b = 0; b < count_; ++b) {
         const InstanceInfo& inf = info_[static_cast<size_t>(b)];
         sh.slices_p = std::max(sh.slices_p, last(at_ctas_, inf.at_cta_end) - first(at_ctas_, inf.at_cta_begin));

@@ -513,10 +513,12 @@ __device__ __forceinline__ void warp_sum(double (&v)[NQ]) {
         for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(kFull, v[q], o);
 }
 
-struct FusedCtl {
-    int active, parity, pending;
+// The trial's snapshot of the control block, three 16-byte words.
+struct alignas(16) FusedCtl {
     double mult_primal, mult_dual, frac;
+    int active, parity, pending, pad;
 };
+static_assert(sizeof(FusedCtl) == 48, "the snapshot travels as three 16-byte words");
 
 template <class T, int V>
 __device__ __forceinline__ double fused_primal(const Global& g, const Work<T>& w, const CtaWork& cw,
@@ -646,6 +648,9 @@ __device__ __forceinline__ void fused_snapshot(const InstanceCtl& c, FusedCtl& f
 }
 
 static_assert(kFusedThreads == kFusedCtaThreads, "the engine sizes clusters by this CTA size");
+// Step factors a fused launch keeps in shared memory (trials past them read
+// the options' table).
+constexpr int kFusedFactors = 160;
 
 // Distributed shared memory of rank `r`: the address of `local` there, and
 // stores of the snapshot's fields.
@@ -659,17 +664,20 @@ __device__ __forceinline__ void st_cluster_i32(uint32_t addr, int v) {
     asm volatile("st.shared::cluster.s32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
 
-// Rank 0's thread 0 writes the next trial's snapshot into every other CTA's
-// copy of `f`; the cluster barrier that follows publishes it.
-__device__ __forceinline__ void fused_publish(const FusedCtl& f, uint32_t C) {
-    for (uint32_t r = 1; r < C; ++r) {
-        const uint32_t a = rank_addr(&f, r);
-        st_cluster_i32(a + offsetof(FusedCtl, active), f.active);
-        st_cluster_i32(a + offsetof(FusedCtl, parity), f.parity);
-        st_cluster_i32(a + offsetof(FusedCtl, pending), f.pending);
-        st_cluster(a + offsetof(FusedCtl, mult_primal), f.mult_primal);
-        st_cluster(a + offsetof(FusedCtl, mult_dual), f.mult_dual);
-        st_cluster(a + offsetof(FusedCtl, frac), f.frac);
+// Lane r in [1, C) of rank 0's first warp copies the snapshot (written by lane
+// 0 before) into CTA r's `f`; the cluster barrier that follows publishes it.
+__device__ __forceinline__ void fused_publish(const FusedCtl& f, uint32_t C, int lane) {
+    __syncwarp();
+    if (lane >= 1 && static_cast<uint32_t>(lane) < C) {
+        const uint32_t a = rank_addr(&f, static_cast<uint32_t>(lane));
+        const int4* w = reinterpret_cast<const int4*>(&f);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const int4 v = w[q];
+            asm volatile("st.shared::cluster.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(a + 16u * q), "r"(v.x),
+                         "r"(v.y), "r"(v.z), "r"(v.w)
+                         : "memory");
+        }
     }
 }
 
@@ -948,6 +956,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
     __shared__ DeviceOptions so;
     __shared__ FusedCtl f;
     __shared__ alignas(16) InstanceCtl sctl;
+    // Rank 0: step_pow entries of iteration indices fac0 .. fac0 + nfac - 1.
+    __shared__ double sfac[2 * kFusedFactors];
+    __shared__ int64_t fac0;
+    __shared__ int nfac;
     extern __shared__ __align__(16) unsigned char fused_smem[];
     double* const part_p = reinterpret_cast<double*>(fused_smem);
     double* const part_d = part_p + fs.slices_p;
@@ -982,6 +994,19 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
         for (int e = threadIdx.x; e < ne_d; e += kFusedThreads) {
             const CtaWork cw = g.a.ctas[inf.a_cta_begin + e];
             tab_d[e] = ((cw.slice_begin - ds0) << 4) | (cw.slice_end - cw.slice_begin);
+        }
+        // The linesearch's step factors of the launch's iteration indices
+        // (one phase per launch: a phase ends at a check, which ends it).
+        {
+            const InstanceCtl& c0 = *cp;
+            const int64_t k0 = c0.phase == kPhasePolish ? c0.polish_iteration : c0.iteration;
+            const int64_t avail = k0 >= 0 && k0 < o.step_pow_entries ? o.step_pow_entries - k0 : 0;
+            const int n = static_cast<int>(avail < kFusedFactors ? avail : kFusedFactors);
+            for (int q = threadIdx.x; q < 2 * n; q += kFusedThreads) sfac[q] = o.step_pow[2 * k0 + q];
+            if (threadIdx.x == 0) {
+                fac0 = k0;
+                nfac = n;
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0) fused_snapshot(sctl, f, kFp64);
@@ -1046,22 +1071,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
     // Remote shared memory is written only once every CTA of the cluster
     // runs: the first snapshot goes out after a barrier.
     cluster_sync_all();
-    if (rank == 0 && threadIdx.x == 0) fused_publish(f, C);
+    if (rank == 0 && threadIdx.x < 32) fused_publish(f, C, lane);
     cluster_sync_all();
     for (int t = 0; t < max_trials; ++t) {
         if (!f.active) break;
-        // The decision's step factors of this trial, loaded while the halves
-        // run.
-        double factors[2] = {0.0, 0.0};
-        bool have_factors = false;
-        if (rank == 0 && threadIdx.x == 0) {
-            const int64_t k = sctl.phase == kPhasePolish ? sctl.polish_iteration : sctl.iteration;
-            if (so.adaptive && k >= 0 && k < so.step_pow_entries) {
-                factors[0] = so.step_pow[2 * k];
-                factors[1] = so.step_pow[2 * k + 1];
-                have_factors = true;
-            }
-        }
         if (with_copies) {
             if (LP.has) {
                 double v[1] = {fused_primal_copies<T, V>(f, LP, cc, C, lane)};
@@ -1120,9 +1133,14 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
         }
         cluster_sync_all();
         if (rank == 0) {
-            fused_entry_totals(tab_p, ne_p, part_p, 1);
-            fused_entry_totals(tab_d, ne_d, part_d, 2);
-            __syncthreads();
+            if (fs.multi) {
+                // (With one slice per entry an entry's total, 0 + its slice's
+                // sum, is that sum: a sum of lane values that start at +0 is
+                // never -0.)
+                fused_entry_totals(tab_p, ne_p, part_p, 1);
+                fused_entry_totals(tab_d, ne_d, part_d, 2);
+                __syncthreads();
+            }
             if (threadIdx.x < 32) {
                 // k_dual's fixed-order sums over the entries' totals
                 // (warp_range_sums3: entries lane, lane + 32, ... in order,
@@ -1135,10 +1153,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
                 }
                 warp_sum<3>(sums);
                 if (threadIdx.x == 0) {
-                    trial_control(sctl, so, sums[0], sums[1], sums[2], inf.n, have_factors ? factors : nullptr);
+                    const int64_t k = sctl.phase == kPhasePolish ? sctl.polish_iteration : sctl.iteration;
+                    const double* fk = k >= fac0 && k - fac0 < nfac ? sfac + 2 * (k - fac0) : nullptr;
+                    trial_control(sctl, so, sums[0], sums[1], sums[2], inf.n, fk);
                     fused_snapshot(sctl, f, kFp64);
-                    fused_publish(f, C);
                 }
+                fused_publish(f, C, lane);
             }
         }
         cluster_sync_all();

@@ -113,6 +113,7 @@ struct FusedShape {
     int32_t entries_p, entries_d;   // most CTA-map entries of an instance per side
     int32_t stage_bytes;            // most bytes of a CTA's staged slices (0: nothing staged)
     int32_t lines;                  // staged with copies: most rows + columns of an instance (else 0)
+    int32_t multi;                  // some CTA-map entry has other than one slice
 };
 // Dynamic shared memory of a fused CTA: one warp sum per primal slice, two
 // per dual slice, one word per CTA-map entry; then, with copies, x and y of
@@ -152,7 +153,7 @@ int fused_max_clusters(int vw, int cluster, const FusedShape& shape);
 constexpr int kFusedCtaThreads = 512;
 // Largest dynamic shared memory the engine gives a fused CTA (its static
 // shared memory, the control block and the options, fit beside it).
-constexpr size_t kFusedMaxSmemHost = 224 * 1024;
+constexpr size_t kFusedMaxSmemHost = 220 * 1024;
 template <class T>
 void launch_check_prep(const Global& g, const Work<T>& w, const DeviceOptions& o, cudaStream_t s);
 void launch_check_spmv(const Global& g, const DeviceOptions& o, int vw, cudaStream_t s);
