@@ -892,7 +892,7 @@ int Engine::timed_position(int k, int slots) const {
 // CTA keeps copies of them and no trial touches global memory.
 void Engine::choose_fused() {
     fused_cluster_ = 0;
-    fused_shape_ = FusedShape{};
+    fused_shape32_ = fused_shape64_ = FusedShape{};
     if (il_ || spec_.ext.two_kernel_trials == 1 || count_ <= 0 || count_ > 16) return;
     // The fused kernel adds an entry's slice sums in slice order; that
     // equals the two-kernel path's block sum (one slice per warp, warps in
@@ -908,6 +908,7 @@ void Engine::choose_fused() {
     auto last = [](const std::vector<CtaWork>& side, int e1) { return side[static_cast<size_t>(e1 - 1)].slice_end; };
     FusedShape sh{};
     sh.multi = multi ? 1 : 0;
+    sh.elem = static_cast<int32_t>(sizeof(double));
     for (int b = 0; b < count_; ++b) {
         const InstanceInfo& inf = info_[static_cast<size_t>(b)];
         sh.slices_p = std::max(sh.slices_p, last(at_ctas_, inf.at_cta_end) - first(at_ctas_, inf.at_cta_begin));
@@ -928,49 +929,58 @@ void Engine::choose_fused() {
     while (cluster < 16 && cluster * warps_per_cta < std::max(sh.slices_p, sh.slices_d)) cluster *= 2;
     if (cluster == 16 && resident(16, sh) <= 0) cluster = 8;
     if (resident(cluster, sh) <= 0) return;
-    if (cluster * warps_per_cta >= std::max(sh.slices_p, sh.slices_d)) {
-        // Staging: CTA rank r's warp q takes slice r * 16 + q of each side;
-        // its bytes at the FP64 element size (the larger of the two stages),
-        // with or without the lines' own iterates.
-        auto stage_bytes = [&](int own_p, int own_d) {
-            int64_t stage = 0;
-            for (int b = 0; b < count_; ++b) {
-                const InstanceInfo& inf = info_[static_cast<size_t>(b)];
-                const MatrixLayout& L = layouts_[spec_.shared_matrix ? 0 : b];
-                const int ps0 = first(at_ctas_, inf.at_cta_begin) - inf.at_slice_base;
-                const int ps1 = last(at_ctas_, inf.at_cta_end) - inf.at_slice_base;
-                const int ds0 = first(a_ctas_, inf.a_cta_begin) - inf.a_slice_base;
-                const int ds1 = last(a_ctas_, inf.a_cta_end) - inf.a_slice_base;
-                for (int r = 0; r < cluster; ++r) {
-                    int64_t cta = 0;
-                    for (int q = 0; q < warps_per_cta; ++q) {
-                        const int k = r * warps_per_cta + q;
-                        if (ps0 + k < ps1)
-                            cta += fused_slice_bytes(L.at.slices[static_cast<size_t>(ps0 + k)].steps,
-                                                     kFusedPrimalConsts + own_p, static_cast<int>(sizeof(double)));
-                        if (ds0 + k < ds1)
-                            cta += fused_slice_bytes(L.a.slices[static_cast<size_t>(ds0 + k)].steps,
-                                                     kFusedDualConsts + own_d, static_cast<int>(sizeof(double)));
-                    }
-                    stage = std::max(stage, cta);
+    // Staging: CTA rank r's warp q takes slice r * 16 + q of each side; its
+    // bytes at element size `elem`, with or without the lines' own iterates.
+    auto stage_bytes = [&](int own_p, int own_d, int elem) {
+        int64_t stage = 0;
+        for (int b = 0; b < count_; ++b) {
+            const InstanceInfo& inf = info_[static_cast<size_t>(b)];
+            const MatrixLayout& L = layouts_[spec_.shared_matrix ? 0 : b];
+            const int ps0 = first(at_ctas_, inf.at_cta_begin) - inf.at_slice_base;
+            const int ps1 = last(at_ctas_, inf.at_cta_end) - inf.at_slice_base;
+            const int ds0 = first(a_ctas_, inf.a_cta_begin) - inf.a_slice_base;
+            const int ds1 = last(a_ctas_, inf.a_cta_end) - inf.a_slice_base;
+            for (int r = 0; r < cluster; ++r) {
+                int64_t cta = 0;
+                for (int q = 0; q < warps_per_cta; ++q) {
+                    const int k = r * warps_per_cta + q;
+                    if (ps0 + k < ps1)
+                        cta += fused_slice_bytes(L.at.slices[static_cast<size_t>(ps0 + k)].steps,
+                                                 kFusedPrimalConsts + own_p, elem);
+                    if (ds0 + k < ds1)
+                        cta += fused_slice_bytes(L.a.slices[static_cast<size_t>(ds0 + k)].steps,
+                                                 kFusedDualConsts + own_d, elem);
                 }
+                stage = std::max(stage, cta);
             }
-            // Never zero when staged (the kernel tells the modes apart by it).
-            return static_cast<int32_t>(std::max<int64_t>(16, std::min<int64_t>(stage, INT32_MAX)));
-        };
-        int32_t lines = 0;
-        for (int b = 0; b < count_; ++b)
-            lines = std::max(lines, info_[static_cast<size_t>(b)].m + info_[static_cast<size_t>(b)].n);
-        FusedShape copies = sh;
-        copies.stage_bytes = stage_bytes(kFusedPrimalOwn, kFusedDualOwn);
+        }
+        // Never zero when staged (the kernel tells the modes apart by it).
+        return static_cast<int32_t>(std::max<int64_t>(16, std::min<int64_t>(stage, INT32_MAX)));
+    };
+    int32_t lines = 0;
+    for (int b = 0; b < count_; ++b)
+        lines = std::max(lines, info_[static_cast<size_t>(b)].m + info_[static_cast<size_t>(b)].n);
+    // Per working precision: copies of x and y if they fit, else the staged
+    // slices if they fit, else neither.
+    auto best = [&](int elem, auto fits) {
+        FusedShape out = sh;
+        out.elem = elem;
+        if (cluster * warps_per_cta < std::max(sh.slices_p, sh.slices_d)) return out;
+        FusedShape copies = out;
+        copies.stage_bytes = stage_bytes(kFusedPrimalOwn, kFusedDualOwn, elem);
         copies.lines = lines;
-        FusedShape staged = sh;
-        staged.stage_bytes = stage_bytes(0, 0);
-        if (fused_smem_bytes(copies) <= kFusedMaxSmemHost && resident(cluster, copies) > 0) sh = copies;
-        else if (fused_smem_bytes(staged) <= kFusedMaxSmemHost && resident(cluster, staged) > 0) sh = staged;
-    }
+        FusedShape staged = out;
+        staged.stage_bytes = stage_bytes(0, 0, elem);
+        if (fused_smem_bytes(copies) <= kFusedMaxSmemHost && fits(copies)) return copies;
+        if (fused_smem_bytes(staged) <= kFusedMaxSmemHost && fits(staged)) return staged;
+        return out;
+    };
+    fused_shape64_ = best(static_cast<int>(sizeof(double)),
+                          [&](const FusedShape& f) { return fused_max_clusters<double>(V, cluster, f) > 0; });
+    if (mixed_)
+        fused_shape32_ = best(static_cast<int>(sizeof(float)),
+                              [&](const FusedShape& f) { return fused_max_clusters<float>(V, cluster, f) > 0; });
     fused_cluster_ = cluster;
-    fused_shape_ = sh;
 }
 
 void Engine::enqueue_chunk(int slots, bool fp64_stage) {
@@ -978,12 +988,11 @@ void Engine::enqueue_chunk(int slots, bool fp64_stage) {
         // One launch runs every instance's trials of the interval.
         const int V = tuning_.vector_width;
         record_timing(0);
-        const FusedShape& sh = fused_shape_;
-        if (mixed_) launch_fused<float>(g_, w32_, dopt_, V, count_, fused_cluster_, slots, sh, stream_);
-        else launch_fused<double>(g_, w64_, dopt_, V, count_, fused_cluster_, slots, sh, stream_);
+        if (mixed_) launch_fused<float>(g_, w32_, dopt_, V, count_, fused_cluster_, slots, fused_shape32_, stream_);
+        else launch_fused<double>(g_, w64_, dopt_, V, count_, fused_cluster_, slots, fused_shape64_, stream_);
         launches_ += 1;
         if (mixed_ && fp64_stage) {
-            launch_fused<double>(g_, w64_, dopt_, V, count_, fused_cluster_, slots, sh, stream_);
+            launch_fused<double>(g_, w64_, dopt_, V, count_, fused_cluster_, slots, fused_shape64_, stream_);
             launches_ += 1;
         }
         record_timing(1);

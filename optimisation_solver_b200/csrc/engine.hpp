@@ -196,7 +196,7 @@ private:
     // kernels per trial slot. Chosen by choose_fused() for one-LP solves and
     // small batches.
     int fused_cluster_ = 0;
-    FusedShape fused_shape_{};   // shared memory of the fused launch
+    FusedShape fused_shape32_{}, fused_shape64_{};   // shared memory of the FP32 / FP64 fused launches
     void choose_fused();
     Interleaved<float> il32_{};
     Interleaved<double> il64_{};

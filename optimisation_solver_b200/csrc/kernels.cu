@@ -1013,7 +1013,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused(Global g, Work<T> w,
     }
     // Staged launches give every warp at most one slice per side; with
     // copies, the x and y of both parities are in every CTA.
-    const bool staged = fs.stage_bytes > 0;
+    const bool staged = fs.stage_bytes > 0 && fs.elem == static_cast<int>(sizeof(T));
     const bool with_copies = staged && fs.lines > 0;
     FusedLane<T> LP{}, LD{};
     FusedCopies<T> cc{};

@@ -114,17 +114,18 @@ struct FusedShape {
     int32_t stage_bytes;            // most bytes of a CTA's staged slices (0: nothing staged)
     int32_t lines;                  // staged with copies: most rows + columns of an instance (else 0)
     int32_t multi;                  // some CTA-map entry has other than one slice
+    int32_t elem;                   // bytes of the launch's working precision
 };
 // Dynamic shared memory of a fused CTA: one warp sum per primal slice, two
 // per dual slice, one word per CTA-map entry; then, with copies, x and y of
-// both parities (sized for FP64); then the staged slices.
+// both parities; then the staged slices.
 __host__ __device__ inline size_t fused_copies_offset(const FusedShape& f) {
     const size_t b = sizeof(double) * (static_cast<size_t>(f.slices_p) + 2 * static_cast<size_t>(f.slices_d)) +
                      sizeof(int32_t) * (static_cast<size_t>(f.entries_p) + static_cast<size_t>(f.entries_d));
     return (b + 15) & ~static_cast<size_t>(15);
 }
 __host__ __device__ inline size_t fused_stage_offset(const FusedShape& f) {
-    return fused_copies_offset(f) + 2 * sizeof(double) * static_cast<size_t>(f.lines);
+    return fused_copies_offset(f) + 2 * static_cast<size_t>(f.elem) * static_cast<size_t>(f.lines);
 }
 __host__ __device__ inline size_t fused_smem_bytes(const FusedShape& f) {
     return fused_stage_offset(f) + static_cast<size_t>(f.stage_bytes);
