@@ -30,6 +30,49 @@ class Lp(C.Structure):
                 ("var_lower", _dp), ("var_upper", _dp)]
 
 
+_i8p = C.POINTER(C.c_int8)
+
+
+class PresolveModel(C.Structure):
+    """pdlpgpu_presolve_model (include/pdlpgpu_presolve.h)."""
+    _fields_ = [("num_variables", C.c_int64), ("num_constraints", C.c_int64),
+                ("var_lower", _dp), ("var_upper", _dp), ("var_type", _i8p),
+                ("row_lower", _dp), ("row_upper", _dp), ("row_start", _i64p),
+                ("row_index", _i32p), ("row_value", _dp), ("objective_offset", C.c_double),
+                ("num_objective_terms", C.c_int64), ("objective_index", _i32p),
+                ("objective_value", _dp), ("num_quadratic_terms", C.c_int64),
+                ("quadratic_index1", _i32p), ("quadratic_index2", _i32p),
+                ("quadratic_value", _dp)]
+
+
+class PresolveResult(C.Structure):
+    """pdlpgpu_presolve_result (include/pdlpgpu_presolve.h)."""
+    _fields_ = [("infeasible", C.c_int32), ("converged", C.c_int32), ("has_maps", C.c_int32),
+                ("original_variables", C.c_int64), ("original_constraints", C.c_int64),
+                ("presolved_variables", C.c_int64), ("presolved_constraints", C.c_int64),
+                ("initial_objective_offset", C.c_double),
+                ("presolved_objective_offset", C.c_double),
+                ("variable_origin", _i64p), ("var_lower", _dp), ("var_upper", _dp),
+                ("constraint_origin", _i64p), ("row_lower", _dp), ("row_upper", _dp),
+                ("row_start", _i64p), ("row_index", _i32p), ("row_value", _dp),
+                ("num_objective_terms", C.c_int64), ("objective_index", _i32p),
+                ("objective_value", _dp), ("num_quadratic_terms", C.c_int64),
+                ("quadratic_index1", _i32p), ("quadratic_index2", _i32p),
+                ("quadratic_value", _dp),
+                ("num_transformations", C.c_int64), ("tr_type", _i32p), ("tr_reason", _i32p),
+                ("tr_index", _i64p), ("tr_variable", _i64p), ("tr_constraint", _i64p),
+                ("tr_old_value", _dp), ("tr_new_value", _dp), ("tr_offset_change", _dp),
+                ("num_fixed", C.c_int64), ("fixed_origin", _i64p), ("fixed_value", _dp),
+                ("fixed_linear", _dp), ("fixed_quadratic_diagonal", _dp),
+                ("fixed_cross_start", _i64p), ("fixed_cross_variable", _i64p),
+                ("fixed_cross_value", _dp),
+                ("num_removed", C.c_int64), ("removed_origin", _i64p), ("removed_lower", _dp),
+                ("removed_upper", _dp), ("removed_reason", _i32p), ("removed_singleton", _i8p),
+                ("removed_singleton_variable", _i64p), ("removed_singleton_coefficient", _dp),
+                ("removed_duplicate", _i8p), ("removed_duplicate_of", _i64p),
+                ("removed_scale", _dp)]
+
+
 class Options(C.Structure):
     _fields_ = [("iteration_limit", C.c_int64), ("time_limit_seconds", C.c_double),
                 ("primal_tolerance", C.c_double), ("dual_tolerance", C.c_double),
@@ -152,6 +195,11 @@ SIGNATURES = {
                                  _i32p, _dp, _i32p, _i32p, _dp]),
     "pdlpgpu_mps_lp": (C.c_int32, [C.c_void_p, C.POINTER(Lp), _i32p]),
     "pdlpgpu_mps_write": (C.c_int32, [C.c_char_p, C.POINTER(Lp), C.c_char_p]),
+    # presolve (include/pdlpgpu_presolve.h)
+    "pdlpgpu_presolve": (C.c_int32, [C.POINTER(PresolveModel),
+                                     C.POINTER(C.POINTER(PresolveResult))]),
+    "pdlpgpu_presolve_free": (None, [C.POINTER(PresolveResult)]),
+    "pdlpgpu_presolve_reason_string": (C.c_char_p, [C.c_int32]),
 }
 
 _LIB = None

@@ -1,12 +1,16 @@
 """ctypes wrapper of oracle/pipeline_shim.cpp -- TEST INFRASTRUCTURE ONLY.
 
-Two builds of the reference's own pipeline (oracle/Makefile, `make pipeline`):
+Builds of the reference's own pipeline (oracle/Makefile):
 
 * ``Pipeline("ref")`` -- oracle/_ref/libpipeline_ref.so, the reference as it is;
 * ``Pipeline("gpu")`` -- oracle/_ref/libpipeline_gpu.so, the same sources with
   the GPU engine's ``pdlp::PdlpSolver::solve`` (include/pdlpgpu_override.hpp)
   linked in place of pdlp_engine/src/pdlp_solver.cpp, so ``solver::solve``
-  reaches the GPU through ``solver::runPdlp`` (src/solver/orchestrator.cpp:337).
+  reaches the GPU through ``solver::runPdlp`` (src/solver/orchestrator.cpp:337);
+* ``Pipeline("fastpre")`` -- oracle/_ref/libpipeline_fastpre.so (`make presolve`),
+  the reference with the library's fast presolve
+  (include/pdlpgpu_presolve_override.hpp) linked in place of
+  src/presolve/presolver.cpp and the reference's own PDLP.
 
 Models come from an MPS file read by the reference ``MpsReader`` or from the
 flat Model IR arrays that ``export`` writes (fixtures travel that way).
@@ -21,7 +25,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBS = {"ref": os.path.join(HERE, "_ref", "libpipeline_ref.so"),
-        "gpu": os.path.join(HERE, "_ref", "libpipeline_gpu.so")}
+        "gpu": os.path.join(HERE, "_ref", "libpipeline_gpu.so"),
+        "fastpre": os.path.join(HERE, "_ref", "libpipeline_fastpre.so")}
 POSTSOLVE_TEST = {"ref": os.path.join(HERE, "_ref", "test_postsolve_integration_ref"),
                   "gpu": os.path.join(HERE, "_ref", "test_postsolve_integration_gpu")}
 

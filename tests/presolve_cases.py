@@ -1,0 +1,171 @@
+"""Seeded presolve models that reach every step of the reference's presolve
+(src/presolve/presolver.cpp): exact and tiny zero coefficients, repeated
+variables in a row and in the objective, fixed and nearly fixed variables,
+empty rows (satisfied and not), singleton rows, rows that tighten bounds,
+redundant rows, exact, scaled, negated and loosened copies of rows,
+contradictory parallel rows, free, half-bounded, integer and binary
+variables, quadratic objective terms. Most models are feasible by
+construction (row bounds placed around the activity of a point inside the
+variable bounds) so that the passes run to their fixed point; some carry a
+planted contradiction.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from optimisation_solver_b200.presolve import BINARY, CONTINUOUS, INTEGER, PresolveModel
+
+INF = np.inf
+
+
+def random_model(seed: int, n: int = 40, m: int = 30, *, integers: bool = False,
+                 quadratic: bool = False, contradiction: bool = False,
+                 copies: float = 0.25, max_row: int = 6) -> PresolveModel:
+    rng = np.random.default_rng(seed)
+    kind = rng.integers(0, 6, n)
+    lo = np.zeros(n)
+    hi = np.full(n, 10.0)
+    vtype = np.zeros(n, np.int8)
+    for j in range(n):
+        k = kind[j]
+        if k == 0:
+            lo[j], hi[j] = 0.0, rng.uniform(1, 20)
+        elif k == 1:
+            lo[j], hi[j] = -INF, rng.uniform(-5, 5)
+        elif k == 2:
+            lo[j], hi[j] = rng.uniform(-5, 5), INF
+        elif k == 3:
+            lo[j], hi[j] = -INF, INF
+        elif k == 4:  # fixed, or fixed to within the tolerance
+            v = float(np.round(rng.uniform(-3, 3), 2))
+            lo[j], hi[j] = v, v + (0.0 if rng.random() < 0.6 else 5e-10)
+        else:
+            lo[j], hi[j] = rng.uniform(-4, 0), rng.uniform(0, 4)
+    if integers:
+        pick = rng.random(n)
+        for j in range(n):
+            if pick[j] < 0.2:
+                vtype[j] = BINARY
+                lo[j], hi[j] = 0.0, 1.0
+            elif pick[j] < 0.4 and np.isfinite(lo[j]) and np.isfinite(hi[j]):
+                vtype[j] = INTEGER
+                lo[j], hi[j] = np.floor(lo[j]), np.ceil(hi[j]) + 1
+    # a point inside the bounds
+    x0 = np.where(np.isfinite(lo), lo, np.where(np.isfinite(hi), hi - 1.0, 0.0))
+    span = np.where(np.isfinite(lo) & np.isfinite(hi), hi - lo, 2.0)
+    x0 = x0 + rng.uniform(0, 1, n) * span * (np.isfinite(lo) & np.isfinite(hi))
+    x0 = np.where(vtype == BINARY, rng.integers(0, 2, n), x0)
+    x0 = np.where(vtype == INTEGER, np.clip(np.round(x0), lo, hi), x0)
+
+    rows_idx, rows_val, rlo, rhi = [], [], [], []
+
+    def add_row(idx, val, act=None, shape=None):
+        idx = np.asarray(idx, np.int32)
+        val = np.asarray(val, np.float64)
+        a = float(val @ x0[idx]) if act is None else act
+        s = rng.integers(0, 5) if shape is None else shape
+        slack = rng.uniform(0.0, 3.0) * (rng.random() < 0.7)
+        if s == 0:
+            b = (a, a)
+        elif s == 1:
+            b = (-INF, a + slack)
+        elif s == 2:
+            b = (a - slack, INF)
+        elif s == 3:
+            b = (a - slack - 1.0, a + slack)
+        else:
+            b = (-INF, INF) if rng.random() < 0.3 else (a - 50.0, a + 50.0)
+        rows_idx.append(idx)
+        rows_val.append(val)
+        rlo.append(b[0])
+        rhi.append(b[1])
+
+    for _ in range(m):
+        r = rng.random()
+        if r < 0.06:  # empty row, usually satisfied
+            rows_idx.append(np.zeros(0, np.int32))
+            rows_val.append(np.zeros(0))
+            ok = rng.random() < 0.9 or contradiction
+            rlo.append(-1.0 if ok else 1.0)
+            rhi.append(1.0 if ok else 2.0)
+            continue
+        length = 1 if r < 0.2 else int(rng.integers(2, max_row + 1))
+        idx = rng.choice(n, size=length, replace=False)
+        val = rng.normal(0, 2, length)
+        if rng.random() < 0.2:
+            val[rng.integers(0, length)] = 0.0 if rng.random() < 0.5 else 1e-12
+        if rng.random() < 0.1 and length > 1:  # a variable twice
+            idx = np.append(idx, idx[0])
+            val = np.append(val, rng.normal())
+        if rng.random() < 0.3:
+            val = np.round(val)
+            val[val == 0] = 1.0
+        add_row(idx, val)
+    # copies of rows: exact, scaled, negated, loosened
+    base = len(rows_idx)
+    for _ in range(int(copies * base)):
+        k = int(rng.integers(0, base))
+        idx, val = rows_idx[k], rows_val[k]
+        if idx.size == 0:
+            continue
+        r = rng.random()
+        s = 1.0 if r < 0.3 else float(rng.choice([2.0, -1.0, 0.5, -3.0, 4.0]))
+        lo_k, hi_k = rlo[k], rhi[k]
+        nlo, nhi = (s * lo_k, s * hi_k) if s > 0 else (s * hi_k, s * lo_k)
+        if r > 0.85:  # loosened: parallel, not a duplicate
+            nlo = nlo - 1.0 if np.isfinite(nlo) else nlo
+        perm = rng.permutation(idx.size)
+        rows_idx.append(idx[perm])
+        rows_val.append(s * val[perm])
+        rlo.append(nlo)
+        rhi.append(nhi)
+    if contradiction:  # a parallel row whose range misses the original's
+        cand = [k for k in range(base) if rows_idx[k].size >= 2 and np.isfinite(rhi[k])]
+        if cand:
+            k = cand[int(rng.integers(0, len(cand)))]
+            rows_idx.append(rows_idx[k].copy())
+            rows_val.append(rows_val[k].copy())
+            rlo.append(rhi[k] + 10.0)
+            rhi.append(rhi[k] + 20.0)
+    order = rng.permutation(len(rows_idx))
+    rows_idx = [rows_idx[k] for k in order]
+    rows_val = [rows_val[k] for k in order]
+    rlo = np.asarray(rlo)[order]
+    rhi = np.asarray(rhi)[order]
+    rs = np.zeros(len(rows_idx) + 1, np.int64)
+    rs[1:] = np.cumsum([r.size for r in rows_idx])
+    ri = np.concatenate(rows_idx) if rows_idx else np.zeros(0, np.int32)
+    rv = np.concatenate(rows_val) if rows_val else np.zeros(0)
+
+    nobj = int(rng.integers(n // 2, n + 1))
+    oi = rng.choice(n, size=nobj, replace=True).astype(np.int32)
+    ov = rng.normal(0, 3, nobj)
+    ov[rng.random(nobj) < 0.1] = 0.0
+    q1 = q2 = np.zeros(0, np.int32)
+    qv = np.zeros(0)
+    if quadratic:
+        nq = int(rng.integers(3, 2 * n))
+        a = rng.integers(0, n, nq).astype(np.int32)
+        b = rng.integers(0, n, nq).astype(np.int32)
+        diag = rng.random(nq) < 0.3
+        b[diag] = a[diag]
+        q1, q2 = np.minimum(a, b), np.maximum(a, b)
+        qv = rng.normal(0, 1, nq)
+        qv[rng.random(nq) < 0.05] = 1e-11
+    return PresolveModel(var_lower=lo, var_upper=hi, var_type=vtype, row_lower=rlo,
+                         row_upper=rhi, row_start=rs, row_index=ri.astype(np.int32),
+                         row_value=rv, objective_index=oi, objective_value=ov,
+                         objective_offset=float(rng.normal()), quadratic_index1=q1,
+                         quadratic_index2=q2, quadratic_value=qv)
+
+
+def flavours(count: int):
+    """`count` models across the flavours, seeded by their position."""
+    out = []
+    for s in range(count):
+        f = s % 6
+        out.append(random_model(
+            1000 + s, n=int(20 + (s * 7) % 90), m=int(10 + (s * 13) % 80),
+            integers=f in (1, 4), quadratic=f in (2, 4), contradiction=f == 3,
+            copies=0.5 if f == 5 else 0.25, max_row=3 if f == 5 else 6))
+    return out

@@ -1,0 +1,159 @@
+"""The fast presolve against the reference's presolve::Presolver::run
+(src/presolve/presolver.cpp), on the CPU (the presolve is host code).
+
+* Committed results (tests/golden/presolve_results.npz, made by
+  tests/golden/make_presolve_golden.py after a field-by-field comparison with
+  the reference): the library reproduces every array bit for bit, with no
+  reference build needed.
+* Where the reference is built (`make -C oracle presolve`): both presolvers
+  on the same model::Model, every field of PresolveResult compared, doubles
+  by their bits -- generated models reaching every step (tests/presolve_cases.py),
+  every MPS file the reference ships that its reader accepts, planted LPs of
+  configuration 0; and solver::solve end to end with the fast presolve linked
+  in place of the reference's, against the reference pipeline.
+* Refused inputs, and a model far beyond what the reference's O(m^2) passes
+  reach in the time the test allows.
+"""
+import glob
+import os
+import time
+
+import numpy as np
+import pytest
+
+import __graft_entry__
+from optimisation_solver_b200 import generators as g
+from optimisation_solver_b200.presolve import PresolveModel, Presolver
+from oracle import presolve_cmp
+from tests import presolve_cases
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden", "presolve_results.npz")
+MODEL_KEYS = ("var_lower", "var_upper", "var_type", "row_lower", "row_upper", "row_start",
+              "row_index", "row_value", "objective_index", "objective_value",
+              "quadratic_index1", "quadratic_index2", "quadratic_value")
+
+needs_reference = pytest.mark.skipif(
+    not presolve_cmp.available(), reason="reference presolver not built (make -C oracle presolve)")
+
+
+@pytest.fixture(scope="module")
+def cmp():
+    return presolve_cmp.PresolveCompare()
+
+
+def bits_equal(a, b) -> bool:
+    a, b = np.asarray(a), np.asarray(b)
+    if a.shape != b.shape:
+        return False
+    if a.dtype.kind == "f" or b.dtype.kind == "f":
+        return np.array_equal(a.astype(np.float64).view(np.int64),
+                              b.astype(np.float64).view(np.int64))
+    return np.array_equal(a, b)
+
+
+def test_golden_results_reproduce_bit_for_bit():
+    from tests.golden.make_presolve_golden import flatten
+    data = np.load(GOLDEN)
+    P = Presolver()
+    for name in data["names"]:
+        name = str(name)
+        m = PresolveModel(**{k: data[f"{name}/model_{k}"] for k in MODEL_KEYS},
+                          objective_offset=float(data[f"{name}/model_objective_offset"]))
+        got = flatten(P.run(m))
+        keys = [k.split("/", 1)[1][len("result_"):] for k in data.files
+                if k.startswith(f"{name}/result_")]
+        assert sorted(keys) == sorted(got), name
+        for k in keys:
+            assert bits_equal(got[k], data[f"{name}/result_{k}"]), (name, k)
+
+
+@needs_reference
+def test_generated_models_match_reference(cmp):
+    seen_infeasible = seen_feasible = 0
+    for k, m in enumerate(presolve_cases.flavours(240)):
+        rc, msg, summary = cmp.compare(m)
+        assert rc == 0, (k, msg)
+        seen_infeasible += summary["infeasible"]
+        seen_feasible += not summary["infeasible"]
+    assert seen_infeasible > 20 and seen_feasible > 20
+
+
+@needs_reference
+def test_reference_mps_files_match_reference(cmp):
+    root = __graft_entry__.REFERENCE_ROOT
+    files = sorted(glob.glob(os.path.join(root, "**", "*.mps"), recursive=True))
+    if not files:
+        pytest.skip("reference MPS files not present")
+    compared = 0
+    for f in files:
+        rc, msg, _ = cmp.compare_mps(f)
+        if rc == -1 and msg.startswith("MpsReader Error"):
+            continue  # files the reference reader itself refuses
+        assert rc == 0, (f, msg)
+        compared += 1
+    assert compared >= 20
+
+
+@needs_reference
+@pytest.mark.parametrize("seed", [1, 2])
+def test_planted_config0_lps_match_reference(cmp, seed):
+    rc, msg, summary = cmp.compare(PresolveModel.from_lp(g.reference_lp(seed).lp))
+    assert rc == 0, msg
+    assert summary["transformations"] > 100 and not summary["infeasible"]
+
+
+@pytest.mark.skipif(not (presolve_cmp.available() and
+                         os.path.exists(os.path.join(os.path.dirname(presolve_cmp.LIB),
+                                                     "libpipeline_fastpre.so"))),
+                    reason="pipelines not built (make -C oracle pipeline presolve)")
+def test_pipeline_with_fast_presolve_matches_reference_pipeline():
+    """solver::solve on the reference's fixture LPs, PDLP forced and the
+    dispatcher's own choice: with the fast presolve linked in place of
+    presolver.cpp every answer is the reference pipeline's, bit for bit."""
+    from oracle.pipeline import Pipeline
+    from tests.test_pipeline import fixture_models
+    ref, fast = Pipeline("ref"), Pipeline("fastpre")
+    for name, d in fixture_models().items():
+        for engine in (0, None):
+            a = ref.import_model(d).solve(engine=engine, tolerance=1e-8)
+            b = fast.import_model(d).solve(engine=engine, tolerance=1e-8)
+            assert (a.status, a.executed_engine, a.iterations) == \
+                (b.status, b.executed_engine, b.iterations), (name, engine)
+            assert bits_equal(a.objective, b.objective), (name, engine)
+            for f in ("x", "duals", "reduced_costs"):
+                assert bits_equal(getattr(a, f), getattr(b, f)), (name, engine, f)
+
+
+def _small_model(**change):
+    m = dict(var_lower=np.zeros(2), var_upper=np.ones(2), row_lower=np.array([0.0]),
+             row_upper=np.array([1.0]), row_start=np.array([0, 2]),
+             row_index=np.array([0, 1], np.int32), row_value=np.array([1.0, 1.0]),
+             objective_index=np.array([0], np.int32), objective_value=np.array([1.0]))
+    m.update(change)
+    return PresolveModel(**m)
+
+
+@pytest.mark.parametrize("change,message", [
+    (dict(row_index=np.array([0, 2], np.int32)), "names no variable"),
+    (dict(row_value=np.array([1.0, np.nan])), "non-finite"),
+    (dict(objective_index=np.array([5], np.int32)), "names no variable"),
+    (dict(var_type=np.array([0, 3], np.int8)), "unknown variable type"),
+    (dict(row_start=np.array([1, 2])), "row_start"),
+])
+def test_refused_inputs(change, message):
+    with pytest.raises(ValueError, match=message):
+        Presolver().run(_small_model(**change))
+
+
+def test_large_model_presolves_in_linear_time():
+    """A planted 20,000 x 40,000 LP: the reference's pairwise row pass alone
+    builds about 2 x 10^8 coefficient maps here; the fast presolve needs well
+    under a second (the bound below is loose on purpose)."""
+    m = PresolveModel.from_lp(g.planted_lp(m=20_000, n=40_000, seed=3).lp)
+    t0 = time.perf_counter()
+    r = Presolver().run(m)
+    elapsed = time.perf_counter() - t0
+    assert not r.infeasible and r.converged
+    assert r.presolved_constraints > 19_000
+    assert elapsed < 20.0, elapsed
