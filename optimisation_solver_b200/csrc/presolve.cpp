@@ -11,6 +11,7 @@
 #include "pdlpgpu_presolve.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -21,6 +22,7 @@
 #include <map>
 #include <new>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -61,6 +63,27 @@ struct Fenwick {
         return s;
     }
 };
+
+// Runs body(begin, end) over [0, n) in contiguous pieces on the host's
+// threads (at most 16; one piece when n is small). Used only for work that
+// reads shared state and writes disjoint outputs, so the results do not
+// depend on the split.
+template <class Body>
+void parallel_for(int64_t n, const Body& body) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int64_t pieces = std::min<int64_t>({static_cast<int64_t>(std::min(hw, 16u)),
+                                              (n + 16383) / 16384, n});
+    if (pieces <= 1) {
+        if (n > 0) body(int64_t{0}, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    pool.reserve(static_cast<std::size_t>(pieces - 1));
+    for (int64_t k = 1; k < pieces; ++k)
+        pool.emplace_back([&, k] { body(n * k / pieces, n * (k + 1) / pieces); });
+    body(int64_t{0}, n / pieces);
+    for (std::thread& t : pool) t.join();
+}
 
 struct FixedRecord {
     int64_t origin = 0;
@@ -112,9 +135,19 @@ private:
     std::vector<double> rv_, lo_, hi_;
     std::vector<char> term_alive_, row_alive_;
     std::vector<int64_t> row_count_;
+    std::vector<char> row_repeats_;  // the row names some variable twice
+    std::vector<double> act_min_, act_max_;
     bool row_zeros_done_ = false;
     // a row lost a term or moved a bound since the duplicate pass last ran
     bool rows_touched_ = true;
+    // Bound tightening's record of its sweeps: a counter of bound changes,
+    // the count at each variable's last change and at each row's last sweep,
+    // whether that sweep moved nothing, and whether the row's own terms or
+    // bounds changed since.
+    int64_t bound_changes_ = 0;
+    std::vector<int64_t> var_changed_, row_swept_;
+    std::vector<char> row_quiet_, row_dirty_;
+    void bound_moved(int64_t v) { var_changed_[v] = ++bound_changes_; }
     // column lists: term positions of each variable, by row then position
     std::vector<int64_t> cs_, cterm_;
     std::vector<int64_t> term_row_;
@@ -230,9 +263,21 @@ Presolve::Presolve(const pdlpgpu_presolve_model& in)
     row_alive_.assign(m, 1);
     row_count_.resize(m);
     term_row_.resize(nnz);
-    for (std::size_t r = 0; r < m; ++r) {
-        row_count_[r] = rs_[r + 1] - rs_[r];
-        for (int64_t p = rs_[r]; p < rs_[r + 1]; ++p) term_row_[p] = static_cast<int64_t>(r);
+    row_repeats_.assign(m, 0);
+    var_changed_.assign(n, 0);
+    row_swept_.assign(m, 0);
+    row_quiet_.assign(m, 0);
+    row_dirty_.assign(m, 1);
+    {
+        std::vector<int64_t> stamp(n, -1);
+        for (std::size_t r = 0; r < m; ++r) {
+            row_count_[r] = rs_[r + 1] - rs_[r];
+            for (int64_t p = rs_[r]; p < rs_[r + 1]; ++p) {
+                term_row_[p] = static_cast<int64_t>(r);
+                if (stamp[ri_[p]] == static_cast<int64_t>(r)) row_repeats_[r] = 1;
+                stamp[ri_[p]] = static_cast<int64_t>(r);
+            }
+        }
     }
     // column lists (counting sort keeps row-then-position order)
     cs_.assign(n + 1, 0);
@@ -304,21 +349,31 @@ bool Presolve::detect_simple_infeasibility() const {
             std::ceil(l - kEps) > std::floor(u + kEps))
             return true;
     }
-    for (int64_t r = 0; r < m_; ++r) {
-        if (!row_alive_[r]) continue;
-        const double l = lo_[r], u = hi_[r];
-        if (std::isnan(l) || std::isnan(u)) return true;
-        if (l > u + kEps) return true;
-        if (row_count_[r] == 0) {
-            if (l > kEps || u < -kEps) return true;
-            continue;
+    // rows: every test reads the model only, so pieces of rows run apart and
+    // the answer is whether any row fails
+    std::atomic<bool> failed{false};
+    parallel_for(m_, [&](int64_t begin, int64_t end) {
+        bool fail = false;
+        for (int64_t r = begin; r < end && !fail; ++r) {
+            if (!row_alive_[r]) continue;
+            const double l = lo_[r], u = hi_[r];
+            if (std::isnan(l) || std::isnan(u) || l > u + kEps) {
+                fail = true;
+                break;
+            }
+            if (row_count_[r] == 0) {
+                if (l > kEps || u < -kEps) fail = true;
+                continue;
+            }
+            double mn, mx;
+            activities(r, mn, mx);
+            if ((std::isfinite(l) && std::isfinite(mx) && mx < l - kEps) ||
+                (std::isfinite(u) && std::isfinite(mn) && mn > u + kEps))
+                fail = true;
         }
-        double mn, mx;
-        activities(r, mn, mx);
-        if (std::isfinite(l) && std::isfinite(mx) && mx < l - kEps) return true;
-        if (std::isfinite(u) && std::isfinite(mn) && mn > u + kEps) return true;
-    }
-    return false;
+        if (fail) failed.store(true, std::memory_order_relaxed);
+    });
+    return failed.load();
 }
 
 // Empty rows (presolver.cpp:1084-1117): highest local index first.
@@ -414,6 +469,7 @@ bool Presolve::fix_variable(int64_t v, double value, int64_t rank) {
             term_alive_[p] = 0;
             row_count_[r]--;
             rows_touched_ = true;
+            row_dirty_[r] = 1;
         }
         if (!row_alive_[r]) continue;
         if (lo_[r] > hi_[r] + kEps) {
@@ -489,6 +545,7 @@ bool Presolve::singleton_row(int64_t r, int64_t rank) {
     }
     const bool lower_changed = !approx_equal(lb_[v], new_lower);
     const bool upper_changed = !approx_equal(ub_[v], new_upper);
+    if (lower_changed || upper_changed) bound_moved(v);
     if (lower_changed) {
         log(PDLPGPU_TR_TIGHTEN_LOWER, PDLPGPU_PR_SINGLETON_LOWER, var_rank_[v], v, r, lb_[v],
             new_lower);
@@ -543,18 +600,28 @@ bool Presolve::tighten_bounds() {
     std::vector<int32_t> tv;
     std::vector<double> ta, cmn, cmx;
     std::vector<char> imn, imx;
-    std::vector<int64_t> stamp(static_cast<std::size_t>(n_), -1);
     for (int64_t r = 0; r < m_; ++r) {
+        // A sweep of a row is a function of the row's terms and bounds and of
+        // its variables' bounds; one that moved nothing, from the same state,
+        // moves nothing again, so such rows are passed over.
         if (!row_alive_[r]) continue;
+        if (row_quiet_[r] && !row_dirty_[r]) {
+            bool fresh = false;
+            for (int64_t p = rs_[r]; p < rs_[r + 1] && !fresh; ++p)
+                fresh = term_alive_[p] && var_changed_[ri_[p]] > row_swept_[r];
+            if (!fresh) continue;
+        }
+        row_dirty_[r] = 0;
+        row_swept_[r] = bound_changes_;
+        const int64_t changes_before = bound_changes_;
         tv.clear();
         ta.clear();
-        bool plain = true;
+        bool plain = !row_repeats_[r];
         for (int64_t p = rs_[r]; p < rs_[r + 1]; ++p) {
             if (!term_alive_[p]) continue;
             tv.push_back(ri_[p]);
             ta.push_back(rv_[p]);
-            if (stamp[ri_[p]] == r || rv_[p] == 0.0) plain = false;
-            stamp[ri_[p]] = r;
+            if (rv_[p] == 0.0) plain = false;
         }
         const std::size_t L = tv.size();
         const double lo = lo_[r], hi = hi_[r];
@@ -576,32 +643,60 @@ bool Presolve::tighten_bounds() {
         };
         if (plain)
             for (std::size_t k = 0; k < L; ++k) contribute(k);
+        // The reference's sum for target t, (((0 + c_0) + c_1) ... + c_{t-1}) +
+        // c_{t+1} ... + c_{L-1}, is the running prefix of the terms before t
+        // (kept exact as the sweep goes, with each term's entry as it stands
+        // after its own turn) continued over the terms after t. A block of
+        // kBlock targets runs its continuations as independent chains, the
+        // block's prefixes taken from the entries as they stand when it
+        // starts; a chain skips a term by adding +0.0, which leaves the sum
+        // unchanged (it starts at +0.0, and a round-to-nearest sum of finite
+        // terms is never -0.0). When a target of the block moves its entry,
+        // the block's later sums are redone from the exact prefix.
+        constexpr std::size_t kBlock = 4;
+        double block_min[kBlock], block_max[kBlock];
+        std::size_t block_start = 0, block_valid = 0;
+        double prefix_min = 0.0, prefix_max = 0.0;  // exact, terms 0 .. t-1
+        auto sum_block = [&](std::size_t t0) {
+            double s0 = prefix_min, u0 = prefix_max;
+            double s1 = s0 + cmn[t0], u1 = u0 + cmx[t0];
+            double s2 = t0 + 1 < L ? s1 + cmn[t0 + 1] : s1, u2 = t0 + 1 < L ? u1 + cmx[t0 + 1] : u1;
+            double s3 = t0 + 2 < L ? s2 + cmn[t0 + 2] : s2, u3 = t0 + 2 < L ? u2 + cmx[t0 + 2] : u2;
+            for (std::size_t k = t0 + 1; k < L; ++k) {
+                const double c1 = cmn[k], c2 = cmx[k];
+                s0 += c1;
+                u0 += c2;
+                s1 += k > t0 + 1 ? c1 : 0.0;
+                u1 += k > t0 + 1 ? c2 : 0.0;
+                s2 += k > t0 + 2 ? c1 : 0.0;
+                u2 += k > t0 + 2 ? c2 : 0.0;
+                s3 += k > t0 + 3 ? c1 : 0.0;
+                u3 += k > t0 + 3 ? c2 : 0.0;
+            }
+            block_min[0] = s0, block_min[1] = s1, block_min[2] = s2, block_min[3] = s3;
+            block_max[0] = u0, block_max[1] = u1, block_max[2] = u2, block_max[3] = u3;
+            block_start = t0;
+            block_valid = std::min(kBlock, L - t0);
+        };
         for (std::size_t t = 0; t < L; ++t) {
             const int32_t v = tv[t];
             const double a = ta[t];
-            if (std::abs(a) <= kEps) continue;
+            if (std::abs(a) <= kEps) {
+                if (plain) {
+                    prefix_min += cmn[t];
+                    prefix_max += cmx[t];
+                }
+                continue;
+            }
             double other_min = 0.0, other_max = 0.0;
             bool min_finite = true, max_finite = true;
             if (plain) {
                 min_finite = n_min_inf - imn[t] == 0;
                 max_finite = n_max_inf - imx[t] == 0;
-                const bool need_min = min_finite && std::isfinite(hi);
-                const bool need_max = max_finite && std::isfinite(lo);
-                if (need_min && need_max) {
-                    for (std::size_t k = 0; k < t; ++k) {
-                        other_min += cmn[k];
-                        other_max += cmx[k];
-                    }
-                    for (std::size_t k = t + 1; k < L; ++k) {
-                        other_min += cmn[k];
-                        other_max += cmx[k];
-                    }
-                } else if (need_min) {
-                    for (std::size_t k = 0; k < t; ++k) other_min += cmn[k];
-                    for (std::size_t k = t + 1; k < L; ++k) other_min += cmn[k];
-                } else if (need_max) {
-                    for (std::size_t k = 0; k < t; ++k) other_max += cmx[k];
-                    for (std::size_t k = t + 1; k < L; ++k) other_max += cmx[k];
+                if ((min_finite && std::isfinite(hi)) || (max_finite && std::isfinite(lo))) {
+                    if (t < block_start || t >= block_start + block_valid) sum_block(t);
+                    other_min = block_min[t - block_start];
+                    other_max = block_max[t - block_start];
                 }
             } else {
                 for (std::size_t k = 0; k < L; ++k) {
@@ -623,6 +718,7 @@ bool Presolve::tighten_bounds() {
             }
             const int8_t type = type_[v];
             const int64_t rank = var_rank_[v];
+            const double lb_before = lb_[v], ub_before = ub_[v];
             if (std::isfinite(lo) && max_finite) {
                 double candidate = (lo - other_max) / a;
                 if (a > 0.0) {
@@ -692,12 +788,22 @@ bool Presolve::tighten_bounds() {
                 infeasible_ = true;
                 return false;
             }
+            if (std::memcmp(&lb_before, &lb_[v], sizeof(double)) != 0 ||
+                std::memcmp(&ub_before, &ub_[v], sizeof(double)) != 0)
+                bound_moved(v);
             if (plain) {
+                const double old_min = cmn[t], old_max = cmx[t];
                 n_min_inf -= imn[t];
                 n_max_inf -= imx[t];
                 contribute(t);
+                if (std::memcmp(&old_min, &cmn[t], sizeof(double)) != 0 ||
+                    std::memcmp(&old_max, &cmx[t], sizeof(double)) != 0)
+                    block_valid = 0;  // later sums of the block included the old entry
+                prefix_min += cmn[t];
+                prefix_max += cmx[t];
             }
         }
+        row_quiet_[r] = bound_changes_ == changes_before;
     }
     return changed;
 }
@@ -705,12 +811,19 @@ bool Presolve::tighten_bounds() {
 // removeRedundantConstraints (presolver.cpp:768-836): highest local index first.
 bool Presolve::redundant_rows() {
     bool changed = false;
+    // no bound moves during this pass: the activities are computed first, in
+    // parallel, then the rows are decided in the reference's order
+    act_min_.resize(static_cast<std::size_t>(m_));
+    act_max_.resize(static_cast<std::size_t>(m_));
+    parallel_for(m_, [&](int64_t begin, int64_t end) {
+        for (int64_t r = begin; r < end; ++r)
+            if (row_alive_[r]) activities(r, act_min_[r], act_max_[r]);
+    });
     int64_t k = alive_rows();
     for (int64_t r = m_ - 1; r >= 0; --r) {
         if (!row_alive_[r]) continue;
         --k;
-        double mn, mx;
-        activities(r, mn, mx);
+        const double mn = act_min_[r], mx = act_max_[r];
         const double lo = lo_[r], hi = hi_[r];
         if (std::isfinite(lo) && std::isfinite(mx) && mx < lo - kEps) {
             infeasible_ = true;
