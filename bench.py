@@ -63,7 +63,8 @@ def parse_args():
                    help="skip the cold-start, plain-GPU and large-LP side measurements")
     p.add_argument("--profile", action="store_true",
                    help="a short cold stream only (for ncu captures of the trial kernels)")
-    p.add_argument("--workload", choices=["flow", "large", "stress", "uneven"], default="flow",
+    p.add_argument("--workload", choices=["flow", "large", "stress", "uneven", "presolve"],
+                   default="flow",
                    help="flow: the headline (config 4); large, stress, uneven: configs 1, 3 and 2, "
                         "each reported on its own line")
     p.add_argument("--count", type=int, default=1024, help="uneven: instances in the batch")
@@ -243,6 +244,11 @@ def main():
 
     if args.impl == "reference":
         return reference_arm(args, world, rank, graph, config)
+    if args.workload == "presolve":
+        # Host code: rank 0 measures it.
+        if rank == 0:
+            print(json.dumps(presolve_workload()))
+        return
     if args.workload in ("large", "stress"):
         # One LP: replicas only, so rank 0 measures it.
         if rank == 0:
@@ -436,6 +442,49 @@ def _planted_instance(args):
     rng = np.random.default_rng(40_000 + i)
     deg = rng.integers(4, 13, size=2 * int(m))
     return g.planted_lp(int(m), 2 * int(m), seed=i, degrees=deg)
+
+
+def presolve_workload() -> dict:
+    """The presolve that solver::solve runs before any engine
+    (src/solver/orchestrator.cpp:596-597): seconds per presolve of planted
+    LPs, the library's (Presolver.run through pdlpgpu_presolve, marshalling
+    included) beside the reference's presolve::Presolver::run (compiled from
+    its sources, oracle/_ref/libpresolve_cmp.so) where the reference finishes
+    in about a minute; the two results are compared field by field on those
+    sizes. Configurations 3 and 1 are timed for the library alone."""
+    from optimisation_solver_b200 import generators as g
+    from optimisation_solver_b200.presolve import PresolveModel, Presolver
+    from oracle import presolve_cmp
+    P = Presolver()
+    rows = []
+    cases = [("planted", 1000, 2000), ("planted", 2000, 4000), ("planted", 4000, 8000),
+             ("stress (config 3)", 100_000, 200_000), ("large (config 1)", 500_000, 1_000_000)]
+    cmp = presolve_cmp.PresolveCompare() if presolve_cmp.available() else None
+    P.run(PresolveModel.from_lp(g.planted_lp(m=200, n=400, seed=1).lp))  # first load untimed
+    for kind, m, n in cases:
+        if kind == "planted":
+            lp = g.planted_lp(m=m, n=n, seed=0).lp
+        else:
+            lp = (g.stress_lp(0) if m == 100_000 else g.large_lp(0)).lp
+        model = PresolveModel.from_lp(lp)
+        t0 = time.perf_counter()
+        r = P.run(model)
+        fast = time.perf_counter() - t0
+        row = {"model": kind, "rows": m, "cols": n, "nnz": int(lp.nnz), "fast_s": round(fast, 4),
+               "presolved_rows": r.presolved_constraints, "presolved_cols": r.presolved_variables,
+               "transformations": int(r.transformations["type"].size),
+               "infeasible": r.infeasible, "converged": r.converged}
+        if cmp is not None and kind == "planted":
+            ref_s, _ = cmp.time(model, "reference")
+            rc, diff, _ = cmp.compare(model)
+            row.update(reference_s=round(ref_s, 3), speedup=round(ref_s / fast, 1),
+                       identical=rc == 0)
+        rows.append(row)
+    return {"workload": "presolve", "metric": "seconds per presolve (presolve::Presolver::run)",
+            "unit": "s", "higher_is_better": False, "data": "synthetic (seeded generators)",
+            "cpu": cpu_model(), "host_threads": os.cpu_count(),
+            "reference": "built from its sources" if cmp is not None else "unavailable",
+            "cases": rows}
 
 
 def side_workload(args, rank: int, world: int, local_rank: int):
