@@ -10,7 +10,9 @@ Builds of the reference's own pipeline (oracle/Makefile):
 * ``Pipeline("fastpre")`` -- oracle/_ref/libpipeline_fastpre.so (`make presolve`),
   the reference with the library's fast presolve
   (include/pdlpgpu_presolve_override.hpp) linked in place of
-  src/presolve/presolver.cpp and the reference's own PDLP.
+  src/presolve/presolver.cpp and the reference's own PDLP;
+* ``Pipeline("gpufast")`` -- oracle/_ref/libpipeline_gpufast.so, both: the fast
+  presolve and the GPU engine behind ``solver::runPdlp``.
 
 Models come from an MPS file read by the reference ``MpsReader`` or from the
 flat Model IR arrays that ``export`` writes (fixtures travel that way).
@@ -26,7 +28,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBS = {"ref": os.path.join(HERE, "_ref", "libpipeline_ref.so"),
         "gpu": os.path.join(HERE, "_ref", "libpipeline_gpu.so"),
-        "fastpre": os.path.join(HERE, "_ref", "libpipeline_fastpre.so")}
+        "fastpre": os.path.join(HERE, "_ref", "libpipeline_fastpre.so"),
+        "gpufast": os.path.join(HERE, "_ref", "libpipeline_gpufast.so")}
 POSTSOLVE_TEST = {"ref": os.path.join(HERE, "_ref", "test_postsolve_integration_ref"),
                   "gpu": os.path.join(HERE, "_ref", "test_postsolve_integration_gpu")}
 

@@ -106,3 +106,52 @@ def test_planted_lp_mps_file_through_gpu_pipeline(tmp_path, gpu_pipeline):
         assert abs(r.objective - planted.objective) <= 1e-6 * abs(planted.objective)
     else:
         assert "violation" in r.message
+
+
+@pytest.mark.skipif(not available("gpufast"), reason="make -C oracle presolve not run")
+def test_fast_presolve_and_gpu_engine_together_match_gpu_pipeline(gpu_pipeline):
+    """Both drop-ins linked at once (the fast presolve in place of
+    presolver.cpp, the engine behind solver::runPdlp): on the reference's
+    fixture LPs every answer is the one of the pipeline with the reference's
+    presolve, bit for bit (same reduced model, same deterministic engine)."""
+    fast = Pipeline("gpufast")
+    for name, d in fixture_models().items():
+        for engine in (ENGINE_PDLP, None):
+            a = gpu_pipeline.import_model(d).solve(engine=engine, tolerance=1e-8)
+            b = fast.import_model(d).solve(engine=engine, tolerance=1e-8)
+            assert (a.status, a.executed_engine, a.iterations) == \
+                (b.status, b.executed_engine, b.iterations), (name, engine)
+            assert np.array_equal(np.float64(a.objective), np.float64(b.objective),
+                                  equal_nan=True), name
+            for f in ("x", "duals", "reduced_costs"):
+                assert np.array_equal(getattr(a, f), getattr(b, f)), (name, engine, f)
+
+
+@pytest.mark.skipif(not available("gpufast"), reason="make -C oracle presolve not run")
+def test_config3_through_solver_solve_with_fast_presolve():
+    """Configuration 3 (100,000 x 200,000, 1.6M nonzeros, rescaled rows and
+    columns, free variables, ranged rows) through the reference's whole
+    solver::solve -- model validation, presolve, dispatch, adapter, the GPU
+    engine, postsolve -- which the reference's own presolve does not finish
+    in practical time (its pairwise row pass). Records the wall time and the
+    outcome."""
+    import time
+    from optimisation_solver_b200.presolve import PresolveModel, Presolver
+    lp = g.stress_lp(0).lp
+    nz = np.flatnonzero(lp.objective)
+    arrays = dict(sense=np.array([0]), offset=np.array([lp.objective_offset]),
+                  objective_index=nz.astype(np.int32), objective_value=lp.objective[nz],
+                  var_type=np.zeros(lp.num_cols, np.int32), var_lower=lp.var_lower,
+                  var_upper=lp.var_upper, row_lower=lp.row_lower, row_upper=lp.row_upper,
+                  row_start=lp.row_start, row_index=lp.col_index, row_value=lp.values)
+    pre = Presolver().run(PresolveModel.from_lp(lp))
+    model = Pipeline("gpufast").import_model(arrays)
+    t0 = time.perf_counter()
+    r = model.solve(engine=ENGINE_PDLP, tolerance=1e-4, threads=os.cpu_count() or 1)
+    wall = time.perf_counter() - t0
+    print(f"config 3 through solver::solve: {r.status} in {wall:.1f} s, {r.iterations} "
+          f"iterations, objective {r.objective:.10g}; {r.message[:120]}")
+    assert r.status not in ("invalid_model", "unsupported"), r.message
+    assert r.executed_engine == ENGINE_PDLP
+    assert not pre.infeasible and pre.presolved_constraints == lp.num_rows
+    assert wall < 600.0
