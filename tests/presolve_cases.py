@@ -20,7 +20,12 @@ INF = np.inf
 
 def random_model(seed: int, n: int = 40, m: int = 30, *, integers: bool = False,
                  quadratic: bool = False, contradiction: bool = False,
-                 copies: float = 0.25, max_row: int = 6) -> PresolveModel:
+                 copies: float = 0.25, max_row: int = 6, exact: bool = False) -> PresolveModel:
+    """exact=True plants no infeasibility: every empty row admits 0, fixed
+    variables are fixed exactly and no row names a variable twice (the
+    reference's bound tightening divides by one of a repeated variable's
+    coefficients, which can cut off feasible points), so large models run to
+    the fixed point."""
     rng = np.random.default_rng(seed)
     kind = rng.integers(0, 6, n)
     lo = np.zeros(n)
@@ -38,7 +43,7 @@ def random_model(seed: int, n: int = 40, m: int = 30, *, integers: bool = False,
             lo[j], hi[j] = -INF, INF
         elif k == 4:  # fixed, or fixed to within the tolerance
             v = float(np.round(rng.uniform(-3, 3), 2))
-            lo[j], hi[j] = v, v + (0.0 if rng.random() < 0.6 else 5e-10)
+            lo[j], hi[j] = v, v + (0.0 if exact or rng.random() < 0.6 else 5e-10)
         else:
             lo[j], hi[j] = rng.uniform(-4, 0), rng.uniform(0, 4)
     if integers:
@@ -85,7 +90,7 @@ def random_model(seed: int, n: int = 40, m: int = 30, *, integers: bool = False,
         if r < 0.06:  # empty row, usually satisfied
             rows_idx.append(np.zeros(0, np.int32))
             rows_val.append(np.zeros(0))
-            ok = rng.random() < 0.9 or contradiction
+            ok = rng.random() < 0.9 or contradiction or exact
             rlo.append(-1.0 if ok else 1.0)
             rhi.append(1.0 if ok else 2.0)
             continue
@@ -94,7 +99,7 @@ def random_model(seed: int, n: int = 40, m: int = 30, *, integers: bool = False,
         val = rng.normal(0, 2, length)
         if rng.random() < 0.2:
             val[rng.integers(0, length)] = 0.0 if rng.random() < 0.5 else 1e-12
-        if rng.random() < 0.1 and length > 1:  # a variable twice
+        if rng.random() < 0.1 and length > 1 and not exact:  # a variable twice
             idx = np.append(idx, idx[0])
             val = np.append(val, rng.normal())
         if rng.random() < 0.3:

@@ -80,6 +80,25 @@ def test_generated_models_match_reference(cmp):
 
 
 @needs_reference
+def test_larger_feasible_models_match_reference(cmp):
+    """Models of a few hundred to 1500 variables with rows up to 40 terms and
+    many copies, feasible by construction, so that the passes run to their
+    fixed point over many rounds."""
+    rng = np.random.default_rng(7)
+    feasible = 0
+    for k in range(12):
+        n, m = int(rng.integers(300, 1500)), int(rng.integers(200, 1000))
+        model = presolve_cases.random_model(
+            60000 + k, n=n, m=m, integers=k % 3 == 1, quadratic=k % 4 == 2,
+            copies=float(rng.choice([0.1, 0.3, 0.6])), max_row=int(rng.choice([6, 12, 40])),
+            exact=True)
+        rc, msg, summary = cmp.compare(model)
+        assert rc == 0, (k, msg)
+        feasible += not summary["infeasible"]
+    assert feasible >= 10
+
+
+@needs_reference
 def test_reference_mps_files_match_reference(cmp):
     root = __graft_entry__.REFERENCE_ROOT
     files = sorted(glob.glob(os.path.join(root, "**", "*.mps"), recursive=True))
@@ -123,6 +142,26 @@ def test_pipeline_with_fast_presolve_matches_reference_pipeline():
             assert bits_equal(a.objective, b.objective), (name, engine)
             for f in ("x", "duals", "reduced_costs"):
                 assert bits_equal(getattr(a, f), getattr(b, f)), (name, engine, f)
+
+
+def test_repeated_variable_tightening_is_the_reference_s():
+    """x + x + y >= 2, x + y <= 1.6, y in [0, 1]: the reference's
+    tightenBounds leaves both x terms out of the other terms' activity and
+    divides by one coefficient, so it sets x >= 1 (0.5 is implied) and then
+    y <= 0.6; the drop-in returns the reference's result, this included."""
+    m = PresolveModel(var_lower=np.array([0.0, 0.0]), var_upper=np.array([10.0, 1.0]),
+                      row_lower=np.array([2.0, -np.inf]), row_upper=np.array([np.inf, 1.6]),
+                      row_start=np.array([0, 3, 5]), row_index=np.array([0, 0, 1, 0, 1], np.int32),
+                      row_value=np.ones(5), objective_index=np.array([0], np.int32),
+                      objective_value=np.array([1.0]))
+    r = Presolver().run(m)
+    t = r.transformations
+    assert t["reason_text"][:3] == ["Constraint tightened variable lower bound",
+                                    "Constraint tightened variable upper bound",
+                                    "Constraint tightened variable upper bound"]
+    assert list(t["variable"][:3]) == [0, 0, 1] and list(t["constraint"][:3]) == [0, 1, 1]
+    assert list(t["new_value"][:3]) == [1.0, 1.6, 1.6 - 1.0]
+    assert list(r.model.var_lower) == [1.0, 0.0]
 
 
 def _small_model(**change):
