@@ -24,10 +24,15 @@
  * alive flags, a fixed variable visits only the rows that hold it (column
  * lists), rows are grouped by their exact support before the pairwise
  * parallel test, and the local indices the log records are recovered with
- * prefix counts. One round costs O(nnz log nnz) plus the reference's own
- * bound-tightening arithmetic (for each term of a row, the activity of the
- * other terms, summed in row order; skipped where two or more other terms are
- * unbounded on that side, which leaves the bound unchanged).
+ * prefix counts. One round costs O(nnz log nnz) plus bound tightening, where
+ * the reference sums, for each term of a row, the activity of the row's
+ * other terms in row order (O(L^2) for a row of L terms): here short rows
+ * run those sums four targets at a time from an exact running prefix, and
+ * rows of 64 terms or more bracket each sum by a proven rounding-error bound
+ * and form it only where the bracket does not already show that the term
+ * moves no bound, so a dense row costs O(L) per round unless its terms
+ * tighten. Rows whose inputs did not change since a sweep that moved nothing
+ * are passed over.
  *
  * Input: a model::Model (include/model/model.h) as arrays. Terms must name
  * existing variables and carry finite values -- what model::Model::validate

@@ -147,6 +147,8 @@ private:
     int64_t bound_changes_ = 0;
     std::vector<int64_t> var_changed_, row_swept_;
     std::vector<char> row_quiet_, row_dirty_;
+    // targets of long rows settled by the bracket, and those summed exactly
+    int64_t long_bracketed_ = 0, long_summed_ = 0;
     void bound_moved(int64_t v) { var_changed_[v] = ++bound_changes_; }
     // column lists: term positions of each variable, by row then position
     std::vector<int64_t> cs_, cterm_;
@@ -678,6 +680,41 @@ bool Presolve::tighten_bounds() {
             block_start = t0;
             block_valid = std::min(kBlock, L - t0);
         };
+        // Long rows: a target's two sums are bracketed instead of formed. The
+        // reference's sequential sum S of the other entries lies within
+        // gamma_(L-2) * sum |c_k| of their exact sum (recursive summation,
+        // round to nearest), and that exact sum is the row's total less the
+        // target's own entry, both taken in extended precision; the bracket
+        // below is wider than that bound by a factor of more than four.
+        // Rounding is monotone, so every candidate the reference can compute
+        // from an S in the bracket lies between the candidates computed from
+        // the bracket's ends: where the extreme one neither moves a bound nor
+        // proves infeasibility, the target does neither, and its sums are not
+        // needed. Otherwise they are formed exactly (the exact prefix
+        // continued over the later entries). The totals are redone whenever
+        // an entry changes.
+        constexpr std::size_t kLongRow = 64;
+        const bool long_row = plain && L >= kLongRow;
+        long double total_min = 0.0L, total_max = 0.0L;
+        double abs_min = 0.0, abs_max = 0.0;
+        auto totals = [&]() {
+            total_min = total_max = 0.0L;
+            abs_min = abs_max = 0.0;
+            for (std::size_t k = 0; k < L; ++k) {
+                total_min += cmn[k];
+                total_max += cmx[k];
+                abs_min += std::abs(cmn[k]);
+                abs_max += std::abs(cmx[k]);
+            }
+        };
+        if (long_row) totals();
+        const double bracket_scale = (static_cast<double>(L) + 8.0) * 0x1p-52;
+        auto bracket = [&](long double total, double absolute, double own, double& s1, double& s2) {
+            const double est = static_cast<double>(total - static_cast<long double>(own));
+            const double b = bracket_scale * (absolute + std::abs(est) + std::abs(own)) + 1e-300;
+            s1 = est - 2.0 * b;
+            s2 = est + 2.0 * b;
+        };
         for (std::size_t t = 0; t < L; ++t) {
             const int32_t v = tv[t];
             const double a = ta[t];
@@ -690,7 +727,47 @@ bool Presolve::tighten_bounds() {
             }
             double other_min = 0.0, other_max = 0.0;
             bool min_finite = true, max_finite = true;
-            if (plain) {
+            bool quiet = false;  // proven to move no bound and prove nothing
+            if (long_row) {
+                min_finite = n_min_inf - imn[t] == 0;
+                max_finite = n_max_inf - imx[t] == 0;
+                const bool need_min = min_finite && std::isfinite(hi);
+                const bool need_max = max_finite && std::isfinite(lo);
+                const double l = lb_[v], u = ub_[v];
+                const int8_t ty = type_[v];
+                quiet = true;
+                if (need_max) {  // candidate (lo - S_max) / a, extreme at S_max's low end
+                    double s1, s2;
+                    bracket(total_max, abs_max, cmx[t], s1, s2);
+                    if (a > 0.0) {
+                        const double c = round_lower((lo - s1) / a, ty);
+                        quiet = std::isfinite(c) && !(c > u + kEps) && !(c > l + kEps);
+                    } else {
+                        const double c = round_upper((lo - s1) / a, ty);
+                        quiet = std::isfinite(c) && !(c < l - kEps) && !(c < u - kEps);
+                    }
+                }
+                if (quiet && need_min) {  // candidate (hi - S_min) / a, extreme at S_min's high end
+                    double s1, s2;
+                    bracket(total_min, abs_min, cmn[t], s1, s2);
+                    if (a > 0.0) {
+                        const double c = round_upper((hi - s2) / a, ty);
+                        quiet = std::isfinite(c) && !(c < l - kEps) && !(c < u - kEps);
+                    } else {
+                        const double c = round_lower((hi - s2) / a, ty);
+                        quiet = std::isfinite(c) && !(c > u + kEps) && !(c > l + kEps);
+                    }
+                }
+                ++(quiet ? long_bracketed_ : long_summed_);
+                if (!quiet) {
+                    other_min = prefix_min;
+                    other_max = prefix_max;
+                    for (std::size_t k = t + 1; k < L; ++k) {
+                        other_min += cmn[k];
+                        other_max += cmx[k];
+                    }
+                }
+            } else if (plain) {
                 min_finite = n_min_inf - imn[t] == 0;
                 max_finite = n_max_inf - imx[t] == 0;
                 if ((min_finite && std::isfinite(hi)) || (max_finite && std::isfinite(lo))) {
@@ -719,7 +796,7 @@ bool Presolve::tighten_bounds() {
             const int8_t type = type_[v];
             const int64_t rank = var_rank_[v];
             const double lb_before = lb_[v], ub_before = ub_[v];
-            if (std::isfinite(lo) && max_finite) {
+            if (!quiet && std::isfinite(lo) && max_finite) {
                 double candidate = (lo - other_max) / a;
                 if (a > 0.0) {
                     candidate = round_lower(candidate, type);
@@ -747,7 +824,7 @@ bool Presolve::tighten_bounds() {
                     }
                 }
             }
-            if (std::isfinite(hi) && min_finite) {
+            if (!quiet && std::isfinite(hi) && min_finite) {
                 double candidate = (hi - other_min) / a;
                 if (a > 0.0) {
                     candidate = round_upper(candidate, type);
@@ -797,8 +874,10 @@ bool Presolve::tighten_bounds() {
                 n_max_inf -= imx[t];
                 contribute(t);
                 if (std::memcmp(&old_min, &cmn[t], sizeof(double)) != 0 ||
-                    std::memcmp(&old_max, &cmx[t], sizeof(double)) != 0)
+                    std::memcmp(&old_max, &cmx[t], sizeof(double)) != 0) {
                     block_valid = 0;  // later sums of the block included the old entry
+                    if (long_row) totals();
+                }
                 prefix_min += cmn[t];
                 prefix_max += cmx[t];
             }
@@ -1053,7 +1132,10 @@ void Presolve::run() {
             if (infeasible_) break;
         }
         lap("duplicate");
-        if (trace) std::fprintf(stderr, "\n");
+        if (trace)
+            std::fprintf(stderr, " long-row targets bracketed/summed %lld/%lld\n",
+                         static_cast<long long>(long_bracketed_),
+                         static_cast<long long>(long_summed_));
         if (!changed) {
             fixed_point = true;
             break;

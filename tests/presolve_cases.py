@@ -174,3 +174,60 @@ def flavours(count: int):
             integers=f in (1, 4), quadratic=f in (2, 4), contradiction=f == 3,
             copies=0.5 if f == 5 else 0.25, max_row=3 if f == 5 else 6))
     return out
+
+
+def long_row_model(seed: int) -> PresolveModel:
+    """Rows of 64 to 400 terms (and some short ones) over a few hundred to
+    2000 variables: equality, one-sided, ranged and loose rows around a point
+    inside the bounds, some with quarter-step coefficients, and on even seeds
+    budget rows over variables bounded at 0 whose right-hand sides are small
+    enough that most of their terms tighten a bound; integer variables on
+    every third seed."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(300, 2000))
+    m = int(rng.integers(20, 120))
+    lo = np.where(rng.random(n) < 0.8, 0.0, rng.uniform(-5, 0, n))
+    hi = np.where(rng.random(n) < 0.9, rng.uniform(1, 20, n), INF)
+    lo[rng.random(n) < 0.03] = -INF
+    vt = np.zeros(n, np.int8)
+    if seed % 3 == 1:
+        ints = rng.random(n) < 0.3
+        vt[ints] = INTEGER
+        lo[ints & np.isfinite(lo)] = np.floor(lo[ints & np.isfinite(lo)])
+        hi[ints & np.isfinite(hi)] = np.ceil(hi[ints & np.isfinite(hi)])
+    box = np.isfinite(hi) & np.isfinite(lo)
+    x0 = np.where(np.isfinite(lo), lo, 0.0) + rng.random(n) * np.where(box, hi - lo, 1.0)
+    x0 = np.where(vt == INTEGER, np.clip(np.round(x0), lo, hi), x0)
+    rows_idx, rows_val, rlo, rhi = [], [], [], []
+    for _ in range(m):
+        length = int(rng.choice([64, 65, 100, 200, 400, 8, 3]))
+        kind = int(rng.integers(0, 5)) if seed % 2 == 0 else int(rng.choice([0, 1, 2, 4]))
+        pool = np.flatnonzero((lo == 0) & np.isfinite(hi)) if kind == 3 else np.arange(n)
+        idx = rng.choice(pool, size=min(length, pool.size), replace=False)
+        val = rng.normal(0, 1, idx.size) if kind != 3 else np.abs(rng.normal(1, 0.2, idx.size))
+        if rng.random() < 0.3:
+            val = np.round(val * 4) / 4
+            val[val == 0] = 0.5
+        act = float(val @ x0[idx])
+        if kind == 0:
+            b = (act, act)
+        elif kind == 1:
+            b = (-INF, act + rng.uniform(0, 2))
+        elif kind == 2:
+            b = (act - rng.uniform(0, 2), INF)
+        elif kind == 3:
+            b = (-INF, rng.uniform(1, 15)) if rng.random() < 0.7 else \
+                (float(np.sum(np.abs(val) * hi[idx])) - rng.uniform(0, 5), INF)
+        else:
+            b = (act - 100.0, act + 100.0)
+        rows_idx.append(idx.astype(np.int32))
+        rows_val.append(val)
+        rlo.append(b[0])
+        rhi.append(b[1])
+    rs = np.zeros(m + 1, np.int64)
+    rs[1:] = np.cumsum([r.size for r in rows_idx])
+    return PresolveModel(var_lower=lo, var_upper=hi, var_type=vt, row_lower=np.array(rlo),
+                         row_upper=np.array(rhi), row_start=rs,
+                         row_index=np.concatenate(rows_idx), row_value=np.concatenate(rows_val),
+                         objective_index=np.arange(n, dtype=np.int32),
+                         objective_value=rng.normal(0, 1, n))

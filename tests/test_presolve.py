@@ -99,6 +99,40 @@ def test_larger_feasible_models_match_reference(cmp):
 
 
 @needs_reference
+def test_long_rows_match_reference(cmp):
+    """Rows of 64 terms and more take the bracketed sums of bound tightening;
+    budget rows make most of their targets tighten (the exact sums), the
+    others stay within their brackets."""
+    feasible = tightened = 0
+    for seed in range(60):
+        rc, msg, summary = cmp.compare(presolve_cases.long_row_model(seed))
+        assert rc == 0, (seed, msg)
+        feasible += not summary["infeasible"]
+        tightened += summary["transformations"]
+    assert feasible >= 20 and tightened > 1000
+
+
+def test_dense_row_presolves_in_linear_time():
+    """One budget row over all 200,000 variables of a planted LP: the
+    reference sums the row's other terms afresh for each of its 200,000
+    terms (4 x 10^10 additions a round); with the bracketed sums the whole
+    presolve takes well under a second (the bound below is loose on purpose)."""
+    lp = g.planted_lp(m=20_000, n=200_000, seed=3).lp
+    n = lp.num_cols
+    m = PresolveModel(var_lower=lp.var_lower, var_upper=lp.var_upper,
+                      row_lower=np.append(lp.row_lower, -np.inf),
+                      row_upper=np.append(lp.row_upper, 0.9 * lp.var_upper.sum()),
+                      row_start=np.append(lp.row_start, lp.row_start[-1] + n),
+                      row_index=np.concatenate([lp.col_index, np.arange(n, dtype=np.int32)]),
+                      row_value=np.concatenate([lp.values, np.ones(n)]),
+                      objective_index=np.arange(n, dtype=np.int32), objective_value=lp.objective)
+    t0 = time.perf_counter()
+    r = Presolver().run(m)
+    assert not r.infeasible and r.converged
+    assert time.perf_counter() - t0 < 20.0
+
+
+@needs_reference
 def test_reference_mps_files_match_reference(cmp):
     root = __graft_entry__.REFERENCE_ROOT
     files = sorted(glob.glob(os.path.join(root, "**", "*.mps"), recursive=True))
