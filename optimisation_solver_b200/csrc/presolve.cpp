@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstdint>
 #include <cstring>
+#include <exception>
 #include <limits>
 #include <map>
 #include <new>
@@ -1331,6 +1332,12 @@ extern "C" int32_t pdlpgpu_presolve(const pdlpgpu_presolve_model* model,
         return 0;
     } catch (const std::bad_alloc&) {
         pdlpgpu_internal_set_error("presolve: out of host memory");
+        return -1;
+    } catch (const std::exception& e) {
+        pdlpgpu_internal_set_error((std::string("presolve: ") + e.what()).c_str());
+        return -1;
+    } catch (...) {
+        pdlpgpu_internal_set_error("presolve: unknown error");
         return -1;
     }
 }
