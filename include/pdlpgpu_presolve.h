@@ -26,12 +26,11 @@
  * parallel test, and the local indices the log records are recovered with
  * prefix counts. One round costs O(nnz log nnz) plus bound tightening, where
  * the reference sums, for each term of a row, the activity of the row's
- * other terms in row order (O(L^2) for a row of L terms): here short rows
- * run those sums four targets at a time from an exact running prefix, and
- * rows of 64 terms or more bracket each sum by a proven rounding-error bound
- * and form it only where the bracket does not already show that the term
- * moves no bound, so a dense row costs O(L) per round unless its terms
- * tighten. Rows whose inputs did not change since a sweep that moved nothing
+ * other terms in row order (O(L^2) for a row of L terms): here each sum is
+ * bracketed by a proven rounding-error bound and formed (from an exact
+ * running prefix) only where the bracket does not already show that the term
+ * moves no bound, so a row costs O(L) per round plus O(L) per term that
+ * tightens. Rows whose inputs did not change since a sweep that moved nothing
  * are passed over.
  *
  * Input: a model::Model (include/model/model.h) as arrays. Terms must name

@@ -11,6 +11,7 @@
 #include "pdlpgpu_presolve.h"
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -73,7 +74,7 @@ template <class Body>
 void parallel_for(int64_t n, const Body& body) {
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     const int64_t pieces = std::min<int64_t>({static_cast<int64_t>(std::min(hw, 16u)),
-                                              (n + 16383) / 16384, n});
+                                              (n + 4095) / 4096, n});
     if (pieces <= 1) {
         if (n > 0) body(int64_t{0}, n);
         return;
@@ -125,7 +126,17 @@ public:
 private:
     // variables
     int64_t n_;
-    std::vector<double> lb_, ub_;
+    // Each variable's bounds side by side ({lower, upper}): bound tightening
+    // reads both for every term it gathers, so they share a cache line.
+    // lb_[v] and ub_[v] name the two halves.
+    template <int Side>
+    struct BoundView {
+        std::vector<std::array<double, 2>>* store;
+        double& operator[](int64_t v) const { return (*store)[static_cast<std::size_t>(v)][Side]; }
+    };
+    std::vector<std::array<double, 2>> bounds_;
+    BoundView<0> lb_{&bounds_};
+    BoundView<1> ub_{&bounds_};
     std::vector<int8_t> type_;
     std::vector<char> var_alive_;
     std::vector<int64_t> var_rank_;
@@ -148,8 +159,8 @@ private:
     int64_t bound_changes_ = 0;
     std::vector<int64_t> var_changed_, row_swept_;
     std::vector<char> row_quiet_, row_dirty_;
-    // targets of long rows settled by the bracket, and those summed exactly
-    int64_t long_bracketed_ = 0, long_summed_ = 0;
+    // tightening targets settled by their brackets, and those summed exactly
+    int64_t bracketed_ = 0, summed_ = 0;
     void bound_moved(int64_t v) { var_changed_[v] = ++bound_changes_; }
     // column lists: term positions of each variable, by row then position
     std::vector<int64_t> cs_, cterm_;
@@ -252,8 +263,8 @@ Presolve::Presolve(const pdlpgpu_presolve_model& in)
     : n_(in.num_variables), m_(in.num_constraints), offset_(in.objective_offset),
       initial_offset_(in.objective_offset) {
     const std::size_t n = static_cast<std::size_t>(n_), m = static_cast<std::size_t>(m_);
-    lb_.assign(in.var_lower, in.var_lower + n);
-    ub_.assign(in.var_upper, in.var_upper + n);
+    bounds_.resize(n);
+    for (std::size_t v = 0; v < n; ++v) bounds_[v] = {in.var_lower[v], in.var_upper[v]};
     type_.assign(in.var_type, in.var_type + n);
     var_alive_.assign(n, 1);
     rs_.assign(in.row_start, in.row_start + m + 1);
@@ -594,10 +605,11 @@ bool Presolve::singleton_rows() {
 // once with their contributions to the row's least and greatest activity
 // (coefficient times the bound the reference multiplies, the same product)
 // and a count of the terms unbounded on each side: a side with an unbounded
-// other term is not finite whatever it adds, so it is not summed, and the
-// finite sums run over contiguous arrays in row order. A term's entries are
-// refreshed after its own bounds may have moved. Rows that name a variable
-// twice, or hold a zero coefficient, take the reference's loop as it stands.
+// other term is not finite whatever it adds. The finite sums are bracketed
+// (below) and formed, in row order, only where the bracket leaves the outcome
+// open. A term's entries are refreshed after its own bounds may have moved.
+// Rows that name a variable twice, or hold a zero coefficient, take the
+// reference's loop as it stands.
 bool Presolve::tighten_bounds() {
     bool changed = false;
     std::vector<int32_t> tv;
@@ -649,39 +661,9 @@ bool Presolve::tighten_bounds() {
         // The reference's sum for target t, (((0 + c_0) + c_1) ... + c_{t-1}) +
         // c_{t+1} ... + c_{L-1}, is the running prefix of the terms before t
         // (kept exact as the sweep goes, with each term's entry as it stands
-        // after its own turn) continued over the terms after t. A block of
-        // kBlock targets runs its continuations as independent chains, the
-        // block's prefixes taken from the entries as they stand when it
-        // starts; a chain skips a term by adding +0.0, which leaves the sum
-        // unchanged (it starts at +0.0, and a round-to-nearest sum of finite
-        // terms is never -0.0). When a target of the block moves its entry,
-        // the block's later sums are redone from the exact prefix.
-        constexpr std::size_t kBlock = 4;
-        double block_min[kBlock], block_max[kBlock];
-        std::size_t block_start = 0, block_valid = 0;
+        // after its own turn) continued over the terms after t.
         double prefix_min = 0.0, prefix_max = 0.0;  // exact, terms 0 .. t-1
-        auto sum_block = [&](std::size_t t0) {
-            double s0 = prefix_min, u0 = prefix_max;
-            double s1 = s0 + cmn[t0], u1 = u0 + cmx[t0];
-            double s2 = t0 + 1 < L ? s1 + cmn[t0 + 1] : s1, u2 = t0 + 1 < L ? u1 + cmx[t0 + 1] : u1;
-            double s3 = t0 + 2 < L ? s2 + cmn[t0 + 2] : s2, u3 = t0 + 2 < L ? u2 + cmx[t0 + 2] : u2;
-            for (std::size_t k = t0 + 1; k < L; ++k) {
-                const double c1 = cmn[k], c2 = cmx[k];
-                s0 += c1;
-                u0 += c2;
-                s1 += k > t0 + 1 ? c1 : 0.0;
-                u1 += k > t0 + 1 ? c2 : 0.0;
-                s2 += k > t0 + 2 ? c1 : 0.0;
-                u2 += k > t0 + 2 ? c2 : 0.0;
-                s3 += k > t0 + 3 ? c1 : 0.0;
-                u3 += k > t0 + 3 ? c2 : 0.0;
-            }
-            block_min[0] = s0, block_min[1] = s1, block_min[2] = s2, block_min[3] = s3;
-            block_max[0] = u0, block_max[1] = u1, block_max[2] = u2, block_max[3] = u3;
-            block_start = t0;
-            block_valid = std::min(kBlock, L - t0);
-        };
-        // Long rows: a target's two sums are bracketed instead of formed. The
+        // A target's two sums are bracketed instead of formed. The
         // reference's sequential sum S of the other entries lies within
         // gamma_(L-2) * sum |c_k| of their exact sum (recursive summation,
         // round to nearest), and that exact sum is the row's total less the
@@ -693,9 +675,8 @@ bool Presolve::tighten_bounds() {
         // proves infeasibility, the target does neither, and its sums are not
         // needed. Otherwise they are formed exactly (the exact prefix
         // continued over the later entries). The totals are redone whenever
-        // an entry changes.
-        constexpr std::size_t kLongRow = 64;
-        const bool long_row = plain && L >= kLongRow;
+        // an entry changes. About one target in twenty moves a bound in a
+        // round of the large configurations; the others cost O(1).
         long double total_min = 0.0L, total_max = 0.0L;
         double abs_min = 0.0, abs_max = 0.0;
         auto totals = [&]() {
@@ -708,7 +689,7 @@ bool Presolve::tighten_bounds() {
                 abs_max += std::abs(cmx[k]);
             }
         };
-        if (long_row) totals();
+        if (plain) totals();
         const double bracket_scale = (static_cast<double>(L) + 8.0) * 0x1p-52;
         auto bracket = [&](long double total, double absolute, double own, double& s1, double& s2) {
             const double est = static_cast<double>(total - static_cast<long double>(own));
@@ -729,7 +710,7 @@ bool Presolve::tighten_bounds() {
             double other_min = 0.0, other_max = 0.0;
             bool min_finite = true, max_finite = true;
             bool quiet = false;  // proven to move no bound and prove nothing
-            if (long_row) {
+            if (plain) {
                 min_finite = n_min_inf - imn[t] == 0;
                 max_finite = n_max_inf - imx[t] == 0;
                 const bool need_min = min_finite && std::isfinite(hi);
@@ -759,7 +740,7 @@ bool Presolve::tighten_bounds() {
                         quiet = std::isfinite(c) && !(c > u + kEps) && !(c > l + kEps);
                     }
                 }
-                ++(quiet ? long_bracketed_ : long_summed_);
+                ++(quiet ? bracketed_ : summed_);
                 if (!quiet) {
                     other_min = prefix_min;
                     other_max = prefix_max;
@@ -767,14 +748,6 @@ bool Presolve::tighten_bounds() {
                         other_min += cmn[k];
                         other_max += cmx[k];
                     }
-                }
-            } else if (plain) {
-                min_finite = n_min_inf - imn[t] == 0;
-                max_finite = n_max_inf - imx[t] == 0;
-                if ((min_finite && std::isfinite(hi)) || (max_finite && std::isfinite(lo))) {
-                    if (t < block_start || t >= block_start + block_valid) sum_block(t);
-                    other_min = block_min[t - block_start];
-                    other_max = block_max[t - block_start];
                 }
             } else {
                 for (std::size_t k = 0; k < L; ++k) {
@@ -875,10 +848,8 @@ bool Presolve::tighten_bounds() {
                 n_max_inf -= imx[t];
                 contribute(t);
                 if (std::memcmp(&old_min, &cmn[t], sizeof(double)) != 0 ||
-                    std::memcmp(&old_max, &cmx[t], sizeof(double)) != 0) {
-                    block_valid = 0;  // later sums of the block included the old entry
-                    if (long_row) totals();
-                }
+                    std::memcmp(&old_max, &cmx[t], sizeof(double)) != 0)
+                    totals();
                 prefix_min += cmn[t];
                 prefix_max += cmx[t];
             }
@@ -1134,9 +1105,9 @@ void Presolve::run() {
         }
         lap("duplicate");
         if (trace)
-            std::fprintf(stderr, " long-row targets bracketed/summed %lld/%lld\n",
-                         static_cast<long long>(long_bracketed_),
-                         static_cast<long long>(long_summed_));
+            std::fprintf(stderr, " targets bracketed/summed %lld/%lld\n",
+                         static_cast<long long>(bracketed_),
+                         static_cast<long long>(summed_));
         if (!changed) {
             fixed_point = true;
             break;
