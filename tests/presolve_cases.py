@@ -231,3 +231,52 @@ def long_row_model(seed: int) -> PresolveModel:
                          row_index=np.concatenate(rows_idx), row_value=np.concatenate(rows_val),
                          objective_index=np.arange(n, dtype=np.int32),
                          objective_value=rng.normal(0, 1, n))
+
+
+def _model(vl, vu, rl, ru, rows, obj=(), vt=None, q=()) -> PresolveModel:
+    rs = np.zeros(len(rows) + 1, np.int64)
+    rs[1:] = np.cumsum([len(r) for r in rows])
+    return PresolveModel(
+        var_lower=np.array(vl, float), var_upper=np.array(vu, float),
+        row_lower=np.array(rl, float), row_upper=np.array(ru, float), row_start=rs,
+        row_index=np.array([i for r in rows for i, _ in r], np.int32),
+        row_value=np.array([v for r in rows for _, v in r], float),
+        objective_index=np.array([i for i, _ in obj], np.int32),
+        objective_value=np.array([v for _, v in obj], float),
+        var_type=None if vt is None else np.array(vt, np.int8),
+        quadratic_index1=np.array([a for a, _, _ in q], np.int32),
+        quadratic_index2=np.array([b for _, b, _ in q], np.int32),
+        quadratic_value=np.array([c for _, _, c in q], float))
+
+
+def edge_models() -> dict:
+    """Small models at the edges of the reference's presolve: nothing at all,
+    no rows, no variables (with a satisfied and an unsatisfiable empty row),
+    every variable fixed, a variable fixed at +inf, fixing with quadratic
+    terms, integer and binary variables with fractional bounds, a NaN bound,
+    coefficients near the top of the double range, a row of zeros, and
+    scaled, negated and parallel copies of a row."""
+    inf = INF
+    return {
+        "empty model": _model([], [], [], [], []),
+        "no rows": _model([0, -inf], [1, inf], [], [], [], obj=[(0, 1.0), (1, -2.0)]),
+        "no variables, empty rows": _model([], [], [-1, 0], [1, 0], [[], []]),
+        "no variables, unsatisfiable empty row": _model([], [], [1], [2], [[]]),
+        "all fixed": _model([1, 2, 3], [1, 2, 3], [0, -inf], [10, 5],
+                            [[(0, 1), (1, 1)], [(1, 1), (2, 1)]], obj=[(0, 1), (2, 4)]),
+        "fixed at +inf": _model([inf, 0], [inf, 1], [-inf], [5], [[(0, 1), (1, 1)]]),
+        "fixed with quadratic terms": _model(
+            [2, 0, -1], [2, 5, 3], [-inf], [4], [[(0, 1), (1, 2), (2, 1)]], obj=[(1, 1)],
+            q=[(0, 0, 1.5), (0, 1, 2.0), (1, 2, -1.0), (0, 2, 3.0)]),
+        "integer with fractional bounds": _model([0.5, 0], [2.5, 1], [1.2], [inf],
+                                                 [[(0, 1), (1, 1)]], vt=[INTEGER, BINARY]),
+        "binary singletons": _model([0, 0], [1, 1], [0.3, -inf], [inf, 0.7],
+                                    [[(0, 1)], [(1, 2)]], vt=[BINARY, BINARY]),
+        "NaN bound": _model([0, np.nan], [1, 1], [-inf], [1], [[(0, 1), (1, 1)]]),
+        "huge coefficients": _model([0, 0], [1e300, 1e300], [-inf], [1e308],
+                                    [[(0, 1e300), (1, 1e300)]]),
+        "row of zeros": _model([0, 0], [1, 1], [-1], [1], [[(0, 0.0), (1, 1e-12)]]),
+        "parallel, scaled, negated": _model(
+            [0, 0], [5, 5], [1, -3, -inf], [2, -1, inf],
+            [[(0, 1), (1, 2)], [(1, -4), (0, -2)], [(0, 3), (1, 6)]]),
+    }

@@ -133,6 +133,13 @@ def test_dense_row_presolves_in_linear_time():
 
 
 @needs_reference
+@pytest.mark.parametrize("name", sorted(presolve_cases.edge_models()))
+def test_edge_models_match_reference(cmp, name):
+    rc, msg, _ = cmp.compare(presolve_cases.edge_models()[name])
+    assert rc == 0, msg
+
+
+@needs_reference
 def test_reference_mps_files_match_reference(cmp):
     root = __graft_entry__.REFERENCE_ROOT
     files = sorted(glob.glob(os.path.join(root, "**", "*.mps"), recursive=True))
