@@ -11,8 +11,10 @@
   every MPS file the reference ships that its reader accepts, planted LPs of
   configuration 0; and solver::solve end to end with the fast presolve linked
   in place of the reference's, against the reference pipeline.
-* Refused inputs, and a model far beyond what the reference's O(m^2) passes
-  reach in the time the test allows.
+* The reference's own presolve and postsolve test programs, built with its
+  presolver and with this one in its place: both pass, with the same output.
+* Refused inputs, and models far beyond what the reference's O(m^2) passes
+  reach in the time the tests allow.
 """
 import glob
 import os
@@ -203,6 +205,40 @@ def test_repeated_variable_tightening_is_the_reference_s():
     assert list(t["variable"][:3]) == [0, 0, 1] and list(t["constraint"][:3]) == [0, 1, 1]
     assert list(t["new_value"][:3]) == [1.0, 1.6, 1.6 - 1.0]
     assert list(r.model.var_lower) == [1.0, 0.0]
+
+
+PRESOLVE_TESTS = os.path.join(os.path.dirname(presolve_cmp.LIB), "presolve_tests")
+REFERENCE_TEST_PROGRAMS = [
+    ("test_batch2", None), ("test_presolve_correctness", None),
+    ("test_transformation_metadata", None), ("test_pipeline_cascades", None),
+    ("test_adversarial", None), ("test_postsolver", None), ("test_presolve_metadata", None),
+] + [("test_dual_reconstruction", case) for case in (
+    "known_shadow_price derived_bound singleton_lower singleton_upper singleton_equality "
+    "singleton_ranged inactive_singleton reduced_costs equality_dual lower_dual upper_dual "
+    "fixed_variable empty_duals wrong_dual_size invalid_constraint_mapping residual_gate "
+    "nonfinite_duals nonfinite_reconstruction quadratic_gradient quadratic_reconstruction "
+    "primal_only missing_bound_provenance invalid_bound_indices invalid_bound_direction "
+    "invalid_source_coefficient invalid_singleton_provenance provenance_after_elimination "
+    "provenance_bound_history derived_bound_directions").split()]
+
+
+@pytest.mark.skipif(not os.path.isdir(PRESOLVE_TESTS),
+                    reason="reference test programs not built (make -C oracle presolve)")
+@pytest.mark.parametrize("program,case", REFERENCE_TEST_PROGRAMS)
+def test_reference_presolve_test_programs_pass_with_fast_presolve(program, case):
+    """The reference's own presolve and postsolve tests (tests/presolve/*.cpp,
+    tests/postsolve/*.cpp, with the cases its CMakeLists.txt registers), built
+    with its presolver and with the fast presolve linked in its place: both
+    pass, and print the same output."""
+    import subprocess
+    args = [case] if case else []
+    ref = subprocess.run([os.path.join(PRESOLVE_TESTS, program + "_ref"), *args],
+                         capture_output=True, text=True, timeout=300)
+    fast = subprocess.run([os.path.join(PRESOLVE_TESTS, program + "_fast"), *args],
+                          capture_output=True, text=True, timeout=300)
+    assert ref.returncode == 0, ref.stdout + ref.stderr
+    assert fast.returncode == 0, fast.stdout + fast.stderr
+    assert fast.stdout == ref.stdout
 
 
 def _small_model(**change):
