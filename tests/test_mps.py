@@ -21,6 +21,8 @@ from optimisation_solver_b200 import generators as g
 from optimisation_solver_b200 import mps
 from oracle.pipeline import Pipeline, available
 
+ROOT_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
 pytestmark = pytest.mark.skipif(not available("ref"),
                                 reason="reference pipeline not built (make -C oracle pipeline)")
 
@@ -404,3 +406,22 @@ def test_parallel_columns_section_reads_the_same(tmp_path, ref):
     bad.write_text(_big_columns_text(error_at=97_531))
     ours, our_error, theirs, their_error = _read_both(ref, str(bad))
     assert their_error is not None and our_error == their_error, (our_error, their_error)
+
+
+def test_reference_mps_reader_tests_pass_with_fast_reader():
+    """The reference's own MPS parser tests (tests/mps/mps_reader_tests.cpp),
+    built with its reader and with the fast reader linked in place of
+    src/mps/mps_reader.cpp (oracle/mps_override.cpp): both pass, with the same
+    output. They read their fixtures relative to the reference root."""
+    import subprocess
+    root = _reference_root()
+    progs = os.path.join(ROOT_DIR, "oracle", "_ref", "presolve_tests")
+    ref_prog = os.path.join(progs, "test_mps_reader_ref")
+    fast_prog = os.path.join(progs, "test_mps_reader_fast")
+    if not (os.path.isdir(os.path.join(root, "tests", "mps")) and os.path.exists(fast_prog)):
+        pytest.skip("reference tree or test programs absent (make -C oracle presolve)")
+    ref = subprocess.run([ref_prog], cwd=root, capture_output=True, text=True, timeout=300)
+    fast = subprocess.run([fast_prog], cwd=root, capture_output=True, text=True, timeout=300)
+    assert ref.returncode == 0, ref.stdout + ref.stderr
+    assert fast.returncode == 0, fast.stdout + fast.stderr
+    assert fast.stdout == ref.stdout
