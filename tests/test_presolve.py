@@ -219,7 +219,12 @@ REFERENCE_TEST_PROGRAMS = [
     "nonfinite_duals nonfinite_reconstruction quadratic_gradient quadratic_reconstruction "
     "primal_only missing_bound_provenance invalid_bound_indices invalid_bound_direction "
     "invalid_source_coefficient invalid_singleton_provenance provenance_after_elimination "
-    "provenance_bound_history derived_bound_directions").split()]
+    "provenance_bound_history derived_bound_directions").split()] + [
+    ("test_classifier_dispatcher", None), ("test_end_to_end", None),
+    ("test_qp_convention", None), ("test_milp_enumeration", None),
+] + [("test_postsolve_integration", case) for case in (
+    "lp_engines qp_signs all_eliminated bound_only integer_models unavailable_duals "
+    "failure_statuses limit_no_solution limit_feasible_solution reduced_api").split()]
 
 
 @pytest.mark.skipif(not os.path.isdir(PRESOLVE_TESTS),
@@ -227,9 +232,12 @@ REFERENCE_TEST_PROGRAMS = [
 @pytest.mark.parametrize("program,case", REFERENCE_TEST_PROGRAMS)
 def test_reference_presolve_test_programs_pass_with_fast_presolve(program, case):
     """The reference's own presolve and postsolve tests (tests/presolve/*.cpp,
-    tests/postsolve/*.cpp, with the cases its CMakeLists.txt registers), built
-    with its presolver and with the fast presolve linked in its place: both
-    pass, and print the same output."""
+    tests/postsolve/*.cpp) and its tests of the whole pipeline
+    (tests/solver, tests/pipeline, tests/qp, tests/milp: classifier and
+    dispatcher, end to end, postsolve integration, the QP convention, 200
+    MILPs against enumeration), with the cases its CMakeLists.txt registers,
+    built with its presolver and with the fast presolve linked in its place:
+    both pass, and print the same output."""
     import subprocess
     args = [case] if case else []
     ref = subprocess.run([os.path.join(PRESOLVE_TESTS, program + "_ref"), *args],
