@@ -249,6 +249,24 @@ def test_reference_presolve_test_programs_pass_with_fast_presolve(program, case)
     assert fast.stdout == ref.stdout
 
 
+@pytest.mark.skipif(not os.path.exists(os.path.join(PRESOLVE_TESTS, "test_cli_fast")),
+                    reason="reference CLI not built (make -C oracle presolve)")
+def test_reference_cli_tests_pass_with_fast_reader_and_presolve():
+    """The reference's command-line program and its own test
+    (tests/cli/test_cli.cpp), built with its MPS reader and presolve and with
+    the fast ones linked in their place: every test passes in both, the same
+    tests in the same order."""
+    import subprocess
+    runs = {k: subprocess.run([os.path.join(PRESOLVE_TESTS, f"test_cli_{k}")],
+                              capture_output=True, text=True, timeout=600)
+            for k in ("ref", "fast")}
+    for k, r in runs.items():
+        assert r.returncode == 0, (k, r.stdout[-2000:] + r.stderr[-2000:])
+    passed = {k: [ln for ln in r.stdout.splitlines() if ln.startswith("[PASSED]")]
+              for k, r in runs.items()}
+    assert passed["fast"] == passed["ref"] and len(passed["ref"]) > 5
+
+
 def _small_model(**change):
     m = dict(var_lower=np.zeros(2), var_upper=np.ones(2), row_lower=np.array([0.0]),
              row_upper=np.array([1.0]), row_start=np.array([0, 2]),
