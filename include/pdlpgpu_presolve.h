@@ -13,23 +13,23 @@
  * number is the one the reference computes: the same passes in the same order
  * (zero coefficients, the infeasibility test, empty rows, fixed variables,
  * singleton rows, bound tightening, redundant rows, duplicate and parallel
- * rows; at most 50 rounds), the same arithmetic in the same order, the same
+ * rows; at most 50 passes), the same arithmetic in the same order, the same
  * early exits with the model as the reference leaves it.
  *
  * What changes is the cost. The reference erases variables and rows from
  * vectors and renumbers every term on each removal, scans every row for each
  * fixed variable, and compares every pair of rows for parallelism (O(m^2)
- * coefficient maps per round, presolver.cpp:906-907), so a model with 10^5
+ * coefficient maps per pass, presolver.cpp:906-907), so a model with 10^5
  * rows does not get through it. Here rows and variables keep stable ids with
  * alive flags, a fixed variable visits only the rows that hold it (column
  * lists), rows are grouped by their exact support before the pairwise
  * parallel test, and the local indices the log records are recovered with
- * prefix counts. One round costs O(nnz log nnz) plus bound tightening, where
+ * prefix counts. One pass costs O(nnz log nnz) plus bound tightening, where
  * the reference sums, for each term of a row, the activity of the row's
  * other terms in row order (O(L^2) for a row of L terms): here each sum is
  * bracketed by a proven rounding-error bound and formed (from an exact
  * running prefix) only where the bracket does not already show that the term
- * moves no bound, so a row costs O(L) per round plus O(L) per term that
+ * moves no bound, so a row costs O(L) per pass plus O(L) per term that
  * tightens. Rows whose inputs did not change since a sweep that moved nothing
  * are passed over.
  *

@@ -322,7 +322,7 @@ Presolve::Presolve(const pdlpgpu_presolve_model& in)
 }
 
 // removeZeroCoefficients (presolver.cpp:128-171). Row coefficients never
-// change after the first round, so their sweep runs once.
+// change after the first pass, so their sweep runs once.
 bool Presolve::remove_zero_coefficients() {
     bool changed = false;
     for (std::size_t k = 0; k < ov_.size(); ++k)
@@ -413,7 +413,7 @@ bool Presolve::empty_rows() {
 
 // fixVariable (presolver.cpp:177-307). Rows that do not hold the variable are
 // not visited: the reference's per-row infeasibility tests cannot fire on them,
-// because every alive row passed the same tests when this round's first
+// because every alive row passed the same tests when this pass's first
 // infeasibility test ran and the empty rows were removed, and a row changes
 // here only when it holds the variable being fixed.
 bool Presolve::fix_variable(int64_t v, double value, int64_t rank) {
@@ -676,7 +676,7 @@ bool Presolve::tighten_bounds() {
         // needed. Otherwise they are formed exactly (the exact prefix
         // continued over the later entries). The totals are redone whenever
         // an entry changes. About one target in twenty moves a bound in a
-        // round of the large configurations; the others cost O(1).
+        // pass of the large configurations; the others cost O(1).
         long double total_min = 0.0L, total_max = 0.0L;
         double abs_min = 0.0, abs_max = 0.0;
         auto totals = [&]() {
@@ -1057,7 +1057,7 @@ void Presolve::run() {
     }
     constexpr int kMaxPasses = 50;
     bool fixed_point = false;
-    // PDLPGPU_PRESOLVE_TRACE=1: one line per round on stderr with the time
+    // PDLPGPU_PRESOLVE_TRACE=1: one line per pass on stderr with the time
     // of each step (ms) and the log's length after it.
     const bool trace = std::getenv("PDLPGPU_PRESOLVE_TRACE") != nullptr;
     using clock = std::chrono::steady_clock;
@@ -1072,7 +1072,7 @@ void Presolve::run() {
     };
     for (int pass = 0; pass < kMaxPasses; ++pass) {
         if (infeasible_) break;
-        if (trace) std::fprintf(stderr, "presolve round %d:", pass);
+        if (trace) std::fprintf(stderr, "presolve pass %d:", pass);
         bool changed = false;
         if (remove_zero_coefficients()) changed = true;
         if (detect_simple_infeasibility()) {

@@ -85,7 +85,7 @@ def test_generated_models_match_reference(cmp):
 def test_larger_feasible_models_match_reference(cmp):
     """Models of a few hundred to 1500 variables with rows up to 40 terms and
     many copies, feasible by construction, so that the passes run to their
-    fixed point over many rounds."""
+    fixed point over many passes."""
     rng = np.random.default_rng(7)
     feasible = 0
     for k in range(12):
@@ -117,7 +117,7 @@ def test_long_rows_match_reference(cmp):
 def test_dense_row_presolves_in_linear_time():
     """One budget row over all 200,000 variables of a planted LP: the
     reference sums the row's other terms afresh for each of its 200,000
-    terms (4 x 10^10 additions a round); with the bracketed sums the whole
+    terms (4 x 10^10 additions a pass); with the bracketed sums the whole
     presolve takes well under a second (the bound below is loose on purpose)."""
     lp = g.planted_lp(m=20_000, n=200_000, seed=3).lp
     n = lp.num_cols
