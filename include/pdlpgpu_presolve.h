@@ -40,7 +40,11 @@
  * do not enter: the log's entity names and the records' names follow from the
  * original indices, and include/pdlpgpu_presolve.hpp fills them in.
  *
- * Host code only: no CUDA call, usable on a host without a GPU.
+ * Host code only: no CUDA call, usable on a host without a GPU. The
+ * read-only steps (the infeasibility test, the rows' activities) of models
+ * above 4096 rows run on up to 16 host threads; PDLPGPU_PRESOLVE_THREADS=k
+ * caps them at k (1: the calling thread only). The result does not depend on
+ * it. PDLPGPU_PRESOLVE_TRACE=1 prints each pass's step times on stderr.
  */
 #ifndef PDLPGPU_PRESOLVE_H
 #define PDLPGPU_PRESOLVE_H

@@ -66,14 +66,23 @@ struct Fenwick {
     }
 };
 
-// Runs body(begin, end) over [0, n) in contiguous pieces on the host's
-// threads (at most 16; one piece when n is small). Used only for work that
-// reads shared state and writes disjoint outputs, so the results do not
-// depend on the split.
+// Host threads the read-only steps may use: PDLPGPU_PRESOLVE_THREADS when set
+// to a positive number (1 runs everything on the calling thread), else the
+// host's hardware threads; at most 16 either way.
+unsigned presolve_threads() {
+    if (const char* v = std::getenv("PDLPGPU_PRESOLVE_THREADS")) {
+        const long k = std::strtol(v, nullptr, 10);
+        if (k > 0) return static_cast<unsigned>(std::min(k, 16L));
+    }
+    return std::min(std::max(1u, std::thread::hardware_concurrency()), 16u);
+}
+
+// Runs body(begin, end) over [0, n) in contiguous pieces of at least 4096 on
+// presolve_threads() threads. Used only for work that reads shared state and
+// writes disjoint outputs, so the results do not depend on the split.
 template <class Body>
 void parallel_for(int64_t n, const Body& body) {
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const int64_t pieces = std::min<int64_t>({static_cast<int64_t>(std::min(hw, 16u)),
+    const int64_t pieces = std::min<int64_t>({static_cast<int64_t>(presolve_threads()),
                                               (n + 4095) / 4096, n});
     if (pieces <= 1) {
         if (n > 0) body(int64_t{0}, n);

@@ -288,6 +288,31 @@ def test_refused_inputs(change, message):
         Presolver().run(_small_model(**change))
 
 
+def test_result_does_not_depend_on_host_threads(tmp_path):
+    """The read-only steps of a 20,000-row model split across threads: one
+    thread (PDLPGPU_PRESOLVE_THREADS=1) and eight give the same result, bit
+    for bit (separate processes: the variable is read at each call)."""
+    import subprocess
+    import sys
+    code = (
+        "import sys, numpy as np\n"
+        "from optimisation_solver_b200 import generators as g\n"
+        "from optimisation_solver_b200.presolve import PresolveModel, Presolver\n"
+        "from tests.golden.make_presolve_golden import flatten\n"
+        "r = flatten(Presolver().run(PresolveModel.from_lp("
+        "g.planted_lp(m=20000, n=40000, seed=3).lp)))\n"
+        "np.savez(sys.argv[1], **{k: np.asarray(v) for k, v in r.items()})\n")
+    root = os.path.dirname(HERE)
+    out = {}
+    for threads in ("1", "8"):
+        path = str(tmp_path / f"threads_{threads}.npz")
+        subprocess.run([sys.executable, "-c", code, path], check=True, cwd=root,
+                       env={**os.environ, "PDLPGPU_PRESOLVE_THREADS": threads,
+                            "PYTHONPATH": root}, timeout=600)
+        out[threads] = np.load(path)
+    assert all(bits_equal(out["1"][k], out["8"][k]) for k in out["1"].files)
+
+
 def test_large_model_presolves_in_linear_time():
     """A planted 20,000 x 40,000 LP: the reference's pairwise row pass alone
     builds about 2 x 10^8 coefficient maps here; the fast presolve needs well
