@@ -26,6 +26,7 @@
 #include <string>
 #include <thread>
 #include <unordered_map>
+#include <utility>
 #include <vector>
 
 extern "C" void pdlpgpu_internal_set_error(const char* message);
@@ -130,7 +131,7 @@ class Presolve {
 public:
     explicit Presolve(const pdlpgpu_presolve_model& in);
     void run();
-    void emit(Out& out) const;
+    void emit(Out& out);  // moves the log out: call once, last
 
 private:
     // variables
@@ -1127,7 +1128,7 @@ void Presolve::run() {
     has_maps_ = true;
 }
 
-void Presolve::emit(Out& o) const {
+void Presolve::emit(Out& o) {
     std::vector<int32_t> rank(static_cast<std::size_t>(n_), -1);
     for (int64_t v = 0; v < n_; ++v)
         if (var_alive_[v]) {
@@ -1160,15 +1161,16 @@ void Presolve::emit(Out& o) const {
             o.qj.push_back(rank[qj_[k]]);
             o.qv.push_back(qv_[k]);
         }
-    const Out& L = logbuf_;
-    o.tr_type_v = L.tr_type_v;
-    o.tr_reason_v = L.tr_reason_v;
-    o.tr_index_v = L.tr_index_v;
-    o.tr_var_v = L.tr_var_v;
-    o.tr_con_v = L.tr_con_v;
-    o.tr_old_v = L.tr_old_v;
-    o.tr_new_v = L.tr_new_v;
-    o.tr_off_v = L.tr_off_v;
+    // the log moves into the result (emit is the last use of this object)
+    Out& L = logbuf_;
+    o.tr_type_v = std::move(L.tr_type_v);
+    o.tr_reason_v = std::move(L.tr_reason_v);
+    o.tr_index_v = std::move(L.tr_index_v);
+    o.tr_var_v = std::move(L.tr_var_v);
+    o.tr_con_v = std::move(L.tr_con_v);
+    o.tr_old_v = std::move(L.tr_old_v);
+    o.tr_new_v = std::move(L.tr_new_v);
+    o.tr_off_v = std::move(L.tr_off_v);
     o.fx_cross_start.push_back(0);
     for (const FixedRecord& f : fixed_) {
         o.fx_origin.push_back(f.origin);
