@@ -5,6 +5,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from optimisation_solver_b200 import native
 from tests import cases
@@ -157,3 +158,20 @@ def test_noalloc_trial_rejects_null_pointers_before_any_launch():
     # x_out NULL with columns present
     rc = lib.pdlpgpu_trial_noalloc(2, 3, *([fake] * 18), 1.0, 1.0, None, fake, fake, fake, None)
     assert rc == -1 and "column-side" in native.last_error()
+
+
+def test_public_c_headers_compile_as_c99(tmp_path):
+    """Every include/*.h is a C header: a C99 translation unit including all
+    of them compiles with warnings as errors, as an FFI binding's would."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    headers = sorted(f for f in os.listdir(INCLUDE) if f.endswith(".h"))
+    src = tmp_path / "all_headers.c"
+    src.write_text("".join(f'#include "{h}"\n' for h in headers) + "int main(void) { return 0; }\n")
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", INCLUDE,
+                        "-c", str(src), "-o", str(tmp_path / "all_headers.o")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
