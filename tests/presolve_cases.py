@@ -280,3 +280,56 @@ def edge_models() -> dict:
             [0, 0], [5, 5], [1, -3, -inf], [2, -1, inf],
             [[(0, 1), (1, 2)], [(1, -4), (0, -2)], [(0, 3), (1, 6)]]),
     }
+
+
+def threshold_model(seed: int, rows: int = 40, width: int = 24) -> PresolveModel:
+    """Rows whose first term's candidate bound lands on the reference's
+    decision threshold (its bound plus or minus 1e-9) to within a few units
+    in the last place: x_t + sum a_k y_k >= lo with y_k in [0, u_k], the
+    other activity summed in the reference's order, and x_t's bound placed
+    at candidate - 1e-9 shifted by -3..3 ulps. Rows share no variables, so
+    each row's outcome is decided on these values alone."""
+    rng = np.random.default_rng(seed)
+    n = rows * (width + 1)
+    lo = np.zeros(n)
+    hi = rng.uniform(0.5, 50.0, n)
+    rlo, rhi, idx_all, val_all = [], [], [], []
+    for r in range(rows):
+        base = r * (width + 1)
+        t = base
+        others = np.arange(base + 1, base + width + 1)
+        a = rng.choice([-1.0, 1.0]) * rng.uniform(0.5, 3.0)
+        c = rng.uniform(0.1, 5.0, width) * rng.choice([-1.0, 1.0], width)
+        lower_side = rng.random() < 0.5
+        bound = float(rng.uniform(-100, 100))
+        # the other terms' extreme activity, summed in row order as the reference does
+        acc = 0.0
+        for k in range(width):
+            if lower_side:   # row >= bound: the others at their largest
+                acc += c[k] * (hi[others[k]] if c[k] > 0 else lo[others[k]])
+            else:            # row <= bound: the others at their smallest
+                acc += c[k] * (lo[others[k]] if c[k] > 0 else hi[others[k]])
+        cand = (bound - acc) / a
+        shift = int(rng.integers(-3, 4))
+        moves_lower = (a > 0) == lower_side
+        if moves_lower:      # the test is cand > lower + 1e-9
+            lo[t] = np.nextafter(cand - 1e-9, np.inf * np.sign(shift)) if shift else cand - 1e-9
+            for _ in range(abs(shift) - 1):
+                lo[t] = np.nextafter(lo[t], np.inf * np.sign(shift))
+            hi[t] = lo[t] + 100.0
+        else:                # the test is cand < upper - 1e-9
+            hi[t] = np.nextafter(cand + 1e-9, np.inf * np.sign(shift)) if shift else cand + 1e-9
+            for _ in range(abs(shift) - 1):
+                hi[t] = np.nextafter(hi[t], np.inf * np.sign(shift))
+            lo[t] = hi[t] - 100.0
+        idx_all.append(np.concatenate([[t], others]).astype(np.int32))
+        val_all.append(np.concatenate([[a], c]))
+        rlo.append(bound if lower_side else -INF)
+        rhi.append(INF if lower_side else bound)
+    rs = np.zeros(rows + 1, np.int64)
+    rs[1:] = np.cumsum([i.size for i in idx_all])
+    return PresolveModel(var_lower=lo, var_upper=hi, row_lower=np.array(rlo),
+                         row_upper=np.array(rhi), row_start=rs,
+                         row_index=np.concatenate(idx_all), row_value=np.concatenate(val_all),
+                         objective_index=np.arange(n, dtype=np.int32),
+                         objective_value=np.ones(n))

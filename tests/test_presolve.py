@@ -135,6 +135,16 @@ def test_dense_row_presolves_in_linear_time():
 
 
 @needs_reference
+def test_threshold_models_match_reference(cmp):
+    """Candidate bounds within a few ulps of the reference's decision
+    threshold (the bound plus or minus 1e-9): the brackets cannot settle these
+    targets and the exact sums decide them as the reference does."""
+    for seed in range(100):
+        rc, msg, _ = cmp.compare(presolve_cases.threshold_model(seed))
+        assert rc == 0, (seed, msg)
+
+
+@needs_reference
 @pytest.mark.parametrize("name", sorted(presolve_cases.edge_models()))
 def test_edge_models_match_reference(cmp, name):
     rc, msg, _ = cmp.compare(presolve_cases.edge_models()[name])
