@@ -4,7 +4,9 @@ through the library's pdlpgpu_presolve (include/pdlpgpu_presolve.h).
 ``Presolver().run(model)`` takes a ``PresolveModel`` (a model::Model as
 arrays) and returns a ``PresolveResult`` holding the reference's result
 fields as numpy arrays: the reduced model, the flags and counts, the
-transformation log with the reference's reason strings, the fixed-variable
+transformation log with reason codes (``reason_text`` maps each code to the
+reference's string; a per-entry list would cost a string per log entry, 15M
+of them on the 500k-row configuration), the fixed-variable
 and removed-constraint records and the index maps (empty when the first
 infeasibility test refused the input, as in the reference). Host code only.
 """
@@ -106,6 +108,7 @@ class PresolveResult:
     transformations: dict
     fixed_variables: dict
     removed_constraints: dict
+    reason_text: dict   # reason code (PDLPGPU_PR_*) -> the reference's text
 
 
 def _arr(ptr, count, dtype):
@@ -146,9 +149,9 @@ class Presolver:
             reduced.var_type = buf.keep["vt"][vo]
             nt, nf, nr = r.num_transformations, r.num_fixed, r.num_removed
             reasons = _arr(r.tr_reason, nt, np.int32)
+            removed_reasons = _arr(r.removed_reason, nr, np.int32)
             text = {int(c): L.pdlpgpu_presolve_reason_string(int(c)).decode()
-                    for c in np.unique(np.concatenate([reasons, _arr(r.removed_reason, nr,
-                                                                     np.int32)]))}
+                    for c in np.unique(np.concatenate([reasons, removed_reasons]))}
             cs = _arr(r.fixed_cross_start, nf + 1, np.int64)
             return PresolveResult(
                 infeasible=bool(r.infeasible), converged=bool(r.converged),
@@ -157,9 +160,9 @@ class Presolver:
                 presolved_constraints=nc, initial_objective_offset=r.initial_objective_offset,
                 presolved_objective_offset=r.presolved_objective_offset, model=reduced,
                 variable_origin=vo, constraint_origin=_arr(r.constraint_origin, nc, np.int64),
+                reason_text=text,
                 transformations=dict(
                     type=_arr(r.tr_type, nt, np.int32), reason=reasons,
-                    reason_text=[text[int(c)] for c in reasons],
                     index=_arr(r.tr_index, nt, np.int64),
                     variable=_arr(r.tr_variable, nt, np.int64),
                     constraint=_arr(r.tr_constraint, nt, np.int64),
@@ -180,7 +183,7 @@ class Presolver:
                     origin=_arr(r.removed_origin, nr, np.int64),
                     lower=_arr(r.removed_lower, nr, np.float64),
                     upper=_arr(r.removed_upper, nr, np.float64),
-                    reason=_arr(r.removed_reason, nr, np.int32),
+                    reason=removed_reasons,
                     singleton=_arr(r.removed_singleton, nr, np.int8),
                     singleton_variable=_arr(r.removed_singleton_variable, nr, np.int64),
                     singleton_coefficient=_arr(r.removed_singleton_coefficient, nr,

@@ -209,9 +209,9 @@ def test_repeated_variable_tightening_is_the_reference_s():
                       objective_value=np.array([1.0]))
     r = Presolver().run(m)
     t = r.transformations
-    assert t["reason_text"][:3] == ["Constraint tightened variable lower bound",
-                                    "Constraint tightened variable upper bound",
-                                    "Constraint tightened variable upper bound"]
+    assert [r.reason_text[int(c)] for c in t["reason"][:3]] == [
+        "Constraint tightened variable lower bound", "Constraint tightened variable upper bound",
+        "Constraint tightened variable upper bound"]
     assert list(t["variable"][:3]) == [0, 0, 1] and list(t["constraint"][:3]) == [0, 1, 1]
     assert list(t["new_value"][:3]) == [1.0, 1.6, 1.6 - 1.0]
     assert list(r.model.var_lower) == [1.0, 0.0]
