@@ -175,3 +175,35 @@ def test_public_c_headers_compile_as_c99(tmp_path):
                         "-c", str(src), "-o", str(tmp_path / "all_headers.o")],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_presolve_refuses_null_arrays_and_bad_counts():
+    """pdlpgpu_presolve checks its arguments before reading them: NULL arrays
+    with positive counts and negative counts return -1 with a message, and
+    nothing is allocated."""
+    lib = native.lib()
+    lower = np.zeros(2)
+    upper = np.ones(2)
+    types = np.zeros(2, np.int8)
+    start = np.array([0], np.int64)
+
+    def call(**kw):
+        f = dict(num_variables=2, num_constraints=0, var_lower=native.ptr(lower),
+                 var_upper=native.ptr(upper), var_type=native.ptr(types, C.c_int8),
+                 row_start=native.ptr(start, C.c_int64))
+        f.update(kw)
+        m = native.PresolveModel(**f)
+        out = C.POINTER(native.PresolveResult)()
+        rc = lib.pdlpgpu_presolve(C.byref(m), C.byref(out))
+        if rc == 0:
+            lib.pdlpgpu_presolve_free(out)
+        return rc, native.last_error()
+
+    assert call()[0] == 0
+    assert call(var_lower=None) == (-1, "presolve: NULL variable array")
+    assert call(row_start=None) == (-1, "presolve: NULL row_start")
+    assert call(num_constraints=1)[0] == -1            # row bounds NULL
+    assert call(num_variables=-1) == (-1, "presolve: negative count")
+    assert call(num_objective_terms=3) == (-1, "presolve: NULL objective array")
+    assert call(num_quadratic_terms=1) == (-1, "presolve: NULL quadratic array")
+    assert lib.pdlpgpu_presolve(None, None) == -1
