@@ -388,6 +388,7 @@ def main():
     achieved = nbytes / (ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": kernel, "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "frac_of_nominal_8000": round(achieved / 8000.0, 4),
                 "traffic": ncu_traffic(kernel), "algorithmic_bytes_per_launch": nbytes,
                 "launch_ms": round(ms, 5), "launch_samples": loop["samples"],
                 "other_kernel": {"name": other, "launch_ms": round(oms, 5),
